@@ -1,0 +1,161 @@
+/*
+ * mgc_b200.h -- C ABI of the B200 DG compressible Euler / Navier-Stokes
+ * right-hand side.
+ *
+ * All array pointers are DEVICE pointers (CUDA global memory) unless the
+ * parameter name ends in _host.  Streams are passed as `void*` (a
+ * cudaStream_t, NULL for the legacy default stream).  Every call is
+ * stream-ordered and asynchronous; none allocates device memory except where
+ * noted.  Return value: 0 on success, a negative MGC_E* code for invalid
+ * arguments or an unsupported configuration; problems found on the device
+ * (NaN, corrupt index, ...) are OR-ed into the caller's `status` word as
+ * MGC_ST* bits and never trap.
+ *
+ * Array layouts (E elements, Np nodes per element, Nc = dim + 2 + nspecies):
+ *   q, rhs        [Nc][E][Np]  float64, field order of ConservedVars:
+ *                 mass, energy, momentum[dim], species_mass[nspecies]
+ *                 (mirgecom/fluid.py:300-312)
+ *   temperature   [E][Np]
+ *   grad          [Nc+1][dim][E][Np]  gradient of q then of temperature
+ *   rx            [E][dim][dim]  dr_r/dx_j
+ *   conn          [E][Nf]  nbr_elem*256 + perm_id, or -(1 + boundary face)
+ *   perm          [nperm][Nfp]  neighbour volume node of own face node m
+ *   bkind         [nbf]  0 = exterior copies interior (DummyBoundary),
+ *                        1 = prescribed exterior state
+ *   bext          [Nc+1][nbf][Nfp]  prescribed exterior q, then temperature
+ */
+#ifndef MGC_B200_H
+#define MGC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGC_OK 0
+#define MGC_E_INVALID (-1)
+#define MGC_E_UNSUPPORTED (-2)
+#define MGC_E_NOT_READY (-3)
+#define MGC_E_CUDA (-4)
+
+#define MGC_ST_NAN 1
+#define MGC_ST_BAD_INDEX 2
+#define MGC_ST_NEWTON_MISS 4
+
+#define MGC_MAX_SPECIES 16
+#define MGC_MAX_REACTIONS 8
+
+#define MGC_EOS_IDEAL 0
+#define MGC_EOS_MIXTURE 1
+#define MGC_TRANSPORT_NONE 0
+#define MGC_TRANSPORT_SIMPLE 1
+#define MGC_TRANSPORT_POWERLAW 2
+#define MGC_FLUX_RUSANOV 0
+#define MGC_FLUX_HLL 1
+#define MGC_FLUX_CENTRAL 2
+
+/* Gas model: GasModel(eos, transport), mirgecom/gas_model.py:82-97, with
+ * IdealSingleGas (mirgecom/eos.py:302), PyrometheusMixture (eos.py:540),
+ * SimpleTransport (mirgecom/transport.py:143), PowerLawTransport (:205). */
+typedef struct {
+  int32_t eos_kind;
+  int32_t nspecies;
+  int32_t niter;            /* Newton iterations, thermochemistry.py:51 */
+  int32_t transport_kind;
+  double gamma, gas_const;
+  double mu, mu_b, kappa;
+  double pl_alpha, pl_beta, pl_sigma, pl_n;
+  int32_t use_lewis;
+  int32_t pad_;
+  double diff[MGC_MAX_SPECIES];
+  double lewis[MGC_MAX_SPECIES];
+  double zero_level;
+} mgc_gas_t;
+
+/* Thermochemistry tables in SI units (pyrometheus conventions). */
+typedef struct {
+  int32_t nspecies, nreactions;
+  double mw[MGC_MAX_SPECIES];
+  double inv_mw[MGC_MAX_SPECIES];
+  double t_mid[MGC_MAX_SPECIES];
+  double a_lo[MGC_MAX_SPECIES][7];
+  double a_hi[MGC_MAX_SPECIES][7];
+  double ord_f[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
+  double nu_p[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
+  double nu_net[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
+  double dnu[MGC_MAX_REACTIONS];
+  double log_a[MGC_MAX_REACTIONS];
+  double beta[MGC_MAX_REACTIONS];
+  double t_act[MGC_MAX_REACTIONS];
+  int32_t reversible[MGC_MAX_REACTIONS];
+} mgc_mechanism_t;
+
+/* Flattened discretization (the host-side replacement of grudge's
+ * DiscretizationCollection connectivity, mirgecom/discretization.py:41-83). */
+typedef struct {
+  int32_t dim, order, nelem, nbf, nperm, pad_;
+  const double* rx;
+  const int32_t* conn;
+  const uint8_t* perm;
+  const int8_t* bkind;
+} mgc_mesh_t;
+
+/* Library version and the list of supported (dim, order) pairs. */
+int mgc_version(void);
+int mgc_supports(int dim, int order, int nspecies, int eos_kind);
+
+/* Upload the reference-element operators of one (dim, order) pair to every
+ * device-side constant bank of the library, on the current device.
+ * weak_host [dim][Np][Np], lift_host [Np][Nf*Nfp], ref_normals_host
+ * [Nf][dim], face_scale_ref_host [Nf], face_nodes_host [Nf][Nfp].
+ * Replaces grudge's reference matrices behind op.weak_local_grad/div,
+ * op.face_mass and op.inverse_mass (mirgecom/operators.py:60-63,92-95). */
+int mgc_upload_reference_operators(int dim, int order, const double* weak_host,
+                                   const double* lift_host,
+                                   const double* ref_normals_host,
+                                   const double* face_scale_ref_host,
+                                   const int32_t* face_nodes_host);
+
+/* Upload a thermochemistry mechanism (pyrometheus class data used by
+ * PyrometheusMixture, mirgecom/eos.py:540-888) on the current device. */
+int mgc_set_mechanism(const mgc_mechanism_t* mech_host);
+
+/* Mixture temperature (mirgecom/eos.py:777-803 -> thermochemistry.py:126-167):
+ * t1 = Newton(e, Y; t_seed), t2 = Newton(e, Y; t1) (t2 may be NULL).
+ * nnodes = E*Np. */
+int mgc_mixture_temperature(int dim, const mgc_gas_t* gas, int64_t nnodes,
+                            const double* q, const double* t_seed, double* t1,
+                            double* t2, void* stream);
+
+/* euler_operator (mirgecom/euler.py:313-416), non-ESDG branch. t_op is the
+ * operator temperature for mixtures (NULL for the ideal gas). */
+int mgc_euler_rhs(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
+                  const double* t_op, const double* bext, int flux_kind,
+                  double* rhs, int32_t* status, void* stream);
+
+/* grad_cv_operator + grad_t_operator (mirgecom/navierstokes.py:129-347). */
+int mgc_ns_grad(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
+                const double* t_op, const double* bext, double* grad,
+                int32_t* status, void* stream);
+
+/* The divergence part of ns_operator (mirgecom/navierstokes.py:533-563) given
+ * the gradients; with add_sources != 0 adds the species source terms
+ * (mirgecom/eos.py:858-875) evaluated at t_src. */
+int mgc_ns_rhs(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
+               const double* t_op, const double* t_src, const double* grad,
+               const double* bext, int flux_kind, int add_sources, double* rhs,
+               int32_t* status, void* stream);
+
+/* One stage of rk4_step (mirgecom/integrators/explicit_rk.py:31-37):
+ * stage 0..2: sum (+)= w k, q_out = q0 + c dt k; stage 3: q_out = q0 +
+ * dt/6 (sum + k).  q_out_lo (float32 copy of q_out) may be NULL. */
+int mgc_rk4_stage(int64_t n, const double* q0, const double* k, double* sum,
+                  double* q_out, float* q_out_lo, int stage, double dt,
+                  void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MGC_B200_H */

@@ -1,0 +1,110 @@
+// Per-translation-unit dispatch from runtime (dim, order, nspecies, eos)
+// to the compiled kernel instantiations.  Each unit that includes this file
+// owns its own constant-memory banks, so it also provides the upload hooks.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "dg_kernels.cuh"
+#include "../../include/mgc_b200.h"
+
+namespace mgc {
+
+static_assert(sizeof(GasParams) == sizeof(mgc_gas_t), "gas struct mismatch");
+static_assert(sizeof(Mechanism) == sizeof(mgc_mechanism_t), "mechanism struct mismatch");
+
+inline int upload_refops_local(int dim, int order, const double* packed64, const float* packed32,
+                               const int* fnodes) {
+  const int off = refops_offset(dim, order);
+  const int n = refops_size(dim, order);
+  const int foff = fnodes_offset(dim, order);
+  const int fn = fnodes_size(dim, order);
+  if (off < 0) return MGC_E_UNSUPPORTED;
+  if (cudaMemcpyToSymbol(c_ref64, packed64, n * sizeof(double), off * sizeof(double)) != cudaSuccess)
+    return MGC_E_CUDA;
+  if (cudaMemcpyToSymbol(c_ref32, packed32, n * sizeof(float), off * sizeof(float)) != cudaSuccess)
+    return MGC_E_CUDA;
+  if (cudaMemcpyToSymbol(c_fnodes, fnodes, fn * sizeof(int), foff * sizeof(int)) != cudaSuccess)
+    return MGC_E_CUDA;
+  return MGC_OK;
+}
+
+inline int upload_mechanism_local(const Mechanism* m) {
+  return cudaMemcpyToSymbol(c_mech, m, sizeof(Mechanism)) == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+}
+
+template <class Kern>
+inline int prepare_kernel(Kern kern, size_t smem) {
+  if (smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return MGC_E_CUDA;
+  }
+  return MGC_OK;
+}
+
+template <class R, int DIM, int ORDER, int NS, bool MIX>
+struct Launch {
+  using C = Cfg<R, DIM, ORDER, NS, MIX>;
+  static size_t smem_grad(int nperm) {
+    return (size_t)C::EPB_GRAD * C::BYTES_GRAD + C::NFN * sizeof(int) + (size_t)nperm * C::NFP + 16;
+  }
+  static size_t smem_rhs(int nperm) {
+    return (size_t)C::EPB_RHS * C::BYTES_RHS + C::NFN * sizeof(int) + (size_t)nperm * C::NFP + 16;
+  }
+  static int grad(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
+    const size_t smem = smem_grad(a.nperm);
+    auto kern = k_grad<R, DIM, ORDER, NS, MIX>;
+    int rc = prepare_kernel(kern, smem);
+    if (rc) return rc;
+    const int nblk = (a.nelem + C::EPB_GRAD - 1) / C::EPB_GRAD;
+    kern<<<nblk, C::NT_GRAD, smem, s>>>(a, g);
+    return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+  }
+  template <bool VISC>
+  static int rhs(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
+    const size_t smem = smem_rhs(a.nperm);
+    auto kern = k_rhs<R, DIM, ORDER, NS, MIX, VISC>;
+    int rc = prepare_kernel(kern, smem);
+    if (rc) return rc;
+    const int nblk = (a.nelem + C::EPB_RHS - 1) / C::EPB_RHS;
+    kern<<<nblk, C::NT_RHS, smem, s>>>(a, g);
+    return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+  }
+};
+
+// op: 0 = grad, 1 = euler rhs, 2 = ns rhs
+template <class R, int DIM, int ORDER>
+inline int dispatch_order(int op, int ns, bool mix, const DGArgs<R>& a, const GasParams& g,
+                          cudaStream_t s) {
+#define MGC_CASE(NSV, MIXV)                                              \
+  if (ns == NSV && mix == MIXV) {                                        \
+    using L = Launch<R, DIM, ORDER, NSV, MIXV>;                          \
+    if (op == 0) return L::grad(a, g, s);                                \
+    if (op == 1) return L::template rhs<false>(a, g, s);                 \
+    return L::template rhs<true>(a, g, s);                               \
+  }
+  MGC_CASE(0, false)
+  MGC_CASE(2, false)
+  MGC_CASE(7, false)
+  MGC_CASE(7, true)
+#undef MGC_CASE
+  return MGC_E_UNSUPPORTED;
+}
+
+inline bool supported_species(int ns, bool mix) {
+  return (ns == 0 && !mix) || (ns == 2 && !mix) || (ns == 7);
+}
+
+template <class R, int DIM>
+inline int mixture_state_dim(int ns, int64_t nnodes, const R* q, const R* tseed, R* t1, R* t2,
+                             const GasParams& g, cudaStream_t s) {
+  if (ns != 7) return MGC_E_UNSUPPORTED;
+  const int nt = 256;
+  int64_t nb = (nnodes + nt - 1) / nt;
+  if (nb > 148 * 16) nb = 148 * 16;
+  if (nb < 1) nb = 1;
+  k_mixture_state<R, DIM, 7><<<(unsigned)nb, nt, 0, s>>>(nnodes, q, tseed, t1, t2, g);
+  return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+}
+
+}  // namespace mgc

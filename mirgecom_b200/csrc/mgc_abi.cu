@@ -1,0 +1,229 @@
+// extern "C" entry points of libmgc_b200 (declared in include/mgc_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <vector>
+
+#include "dg_dispatch.cuh"
+
+namespace mgc {
+int tu2_upload_refops(int, int, const double*, const float*, const int*);
+int tu3_upload_refops(int, int, const double*, const float*, const int*);
+int tu2_upload_mechanism(const Mechanism*);
+int tu3_upload_mechanism(const Mechanism*);
+int tu2_dispatch(int, int, int, bool, const DGArgs<double>&, const GasParams&, cudaStream_t);
+int tu3_dispatch(int, int, int, bool, const DGArgs<double>&, const GasParams&, cudaStream_t);
+int tu2_mixture_state(int, int64_t, const double*, const double*, double*, double*,
+                      const GasParams&, cudaStream_t);
+int tu3_mixture_state(int, int64_t, const double*, const double*, double*, double*,
+                      const GasParams&, cudaStream_t);
+}  // namespace mgc
+
+using namespace mgc;
+
+namespace {
+
+// per-device record of which reference operators / mechanism were uploaded
+constexpr int kMaxDevices = 64;
+bool g_refops_ready[kMaxDevices][8] = {};
+bool g_mech_ready[kMaxDevices] = {};
+
+int current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) return -1;
+  return d;
+}
+
+bool mesh_ok(const mgc_mesh_t* m) {
+  return m && (m->dim == 2 || m->dim == 3) && m->nelem > 0 && m->rx && m->conn &&
+         m->nperm > 0 && m->nperm <= 256 && m->perm && m->nbf >= 0 &&
+         (m->nbf == 0 || m->bkind) && (int64_t)m->nelem * 256 < (int64_t)1 << 31;
+}
+
+bool gas_ok(const mgc_gas_t* g) {
+  return g && (g->eos_kind == MGC_EOS_IDEAL || g->eos_kind == MGC_EOS_MIXTURE) &&
+         g->nspecies >= 0 && g->nspecies <= MGC_MAX_SPECIES && g->niter >= 0;
+}
+
+int ready(const mgc_mesh_t* m, const mgc_gas_t* g) {
+  const int dev = current_device();
+  if (dev < 0) return MGC_E_CUDA;
+  const int slot = refops_slot(m->dim, m->order);
+  if (slot < 0) return MGC_E_UNSUPPORTED;
+  if (!g_refops_ready[dev][slot]) return MGC_E_NOT_READY;
+  if (g->eos_kind == MGC_EOS_MIXTURE && !g_mech_ready[dev]) return MGC_E_NOT_READY;
+  return MGC_OK;
+}
+
+DGArgs<double> make_args(const mgc_mesh_t* m, const double* q, const double* t_op,
+                         const double* t_src, const double* grad, double* out,
+                         const double* bext, int flux_kind, int add_sources, int32_t* status) {
+  DGArgs<double> a;
+  std::memset(&a, 0, sizeof(a));
+  a.nelem = m->nelem;
+  a.nbf = m->nbf;
+  a.nperm = m->nperm;
+  a.flux_kind = flux_kind;
+  a.q = q;
+  a.t_op = t_op;
+  a.t_src = t_src;
+  a.grad = grad;
+  a.out = out;
+  a.rx = m->rx;
+  a.conn = m->conn;
+  a.perm = m->perm;
+  a.bkind = m->bkind;
+  a.bext = bext;
+  a.status = status;
+  a.add_sources = add_sources;
+  return a;
+}
+
+GasParams to_params(const mgc_gas_t* g) {
+  GasParams p;
+  std::memcpy(&p, g, sizeof(p));
+  return p;
+}
+
+int dispatch(int op, const mgc_mesh_t* m, const mgc_gas_t* g, const DGArgs<double>& a,
+             cudaStream_t s) {
+  const bool mix = g->eos_kind == MGC_EOS_MIXTURE;
+  if (!supported_species(g->nspecies, mix)) return MGC_E_UNSUPPORTED;
+  const GasParams p = to_params(g);
+  if (m->dim == 2) return tu2_dispatch(op, m->order, g->nspecies, mix, a, p, s);
+  return tu3_dispatch(op, m->order, g->nspecies, mix, a, p, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mgc_version(void) { return 1; }
+
+int mgc_supports(int dim, int order, int nspecies, int eos_kind) {
+  if (refops_slot(dim, order) < 0) return 0;
+  return supported_species(nspecies, eos_kind == MGC_EOS_MIXTURE) ? 1 : 0;
+}
+
+int mgc_upload_reference_operators(int dim, int order, const double* weak_host,
+                                   const double* lift_host, const double* ref_normals_host,
+                                   const double* face_scale_ref_host,
+                                   const int32_t* face_nodes_host) {
+  const int slot = refops_slot(dim, order);
+  if (slot < 0) return MGC_E_UNSUPPORTED;
+  if (!weak_host || !lift_host || !ref_normals_host || !face_scale_ref_host || !face_nodes_host)
+    return MGC_E_INVALID;
+  const int np = simplex_npts(dim, order);
+  const int nf = dim + 1;
+  const int nfp = simplex_npts(dim - 1, order);
+  const int n = refops_size(dim, order);
+  std::vector<double> p64(n);
+  int o = 0;
+  for (int i = 0; i < dim * np * np; ++i) p64[o++] = weak_host[i];
+  for (int i = 0; i < np * nf * nfp; ++i) p64[o++] = lift_host[i];
+  for (int i = 0; i < nf * dim; ++i) p64[o++] = ref_normals_host[i];
+  for (int i = 0; i < nf; ++i) p64[o++] = face_scale_ref_host[i];
+  std::vector<float> p32(n);
+  for (int i = 0; i < n; ++i) p32[i] = (float)p64[i];
+  std::vector<int> fn(nf * nfp);
+  for (int i = 0; i < nf * nfp; ++i) {
+    if (face_nodes_host[i] < 0 || face_nodes_host[i] >= np) return MGC_E_INVALID;
+    fn[i] = face_nodes_host[i];
+  }
+  int rc = tu2_upload_refops(dim, order, p64.data(), p32.data(), fn.data());
+  if (rc) return rc;
+  rc = tu3_upload_refops(dim, order, p64.data(), p32.data(), fn.data());
+  if (rc) return rc;
+  rc = upload_refops_local(dim, order, p64.data(), p32.data(), fn.data());
+  if (rc) return rc;
+  const int dev = current_device();
+  if (dev < 0) return MGC_E_CUDA;
+  g_refops_ready[dev][slot] = true;
+  return MGC_OK;
+}
+
+int mgc_set_mechanism(const mgc_mechanism_t* mech_host) {
+  if (!mech_host || mech_host->nspecies < 1 || mech_host->nspecies > MGC_MAX_SPECIES ||
+      mech_host->nreactions < 0 || mech_host->nreactions > MGC_MAX_REACTIONS)
+    return MGC_E_INVALID;
+  Mechanism m;
+  std::memcpy(&m, mech_host, sizeof(m));
+  int rc = tu2_upload_mechanism(&m);
+  if (rc) return rc;
+  rc = tu3_upload_mechanism(&m);
+  if (rc) return rc;
+  rc = upload_mechanism_local(&m);
+  if (rc) return rc;
+  const int dev = current_device();
+  if (dev < 0) return MGC_E_CUDA;
+  g_mech_ready[dev] = true;
+  return MGC_OK;
+}
+
+int mgc_mixture_temperature(int dim, const mgc_gas_t* gas, int64_t nnodes, const double* q,
+                            const double* t_seed, double* t1, double* t2, void* stream) {
+  if (!gas_ok(gas) || gas->eos_kind != MGC_EOS_MIXTURE || nnodes < 0 || !q || !t_seed || !t1)
+    return MGC_E_INVALID;
+  if (nnodes == 0) return MGC_OK;
+  const int dev = current_device();
+  if (dev < 0) return MGC_E_CUDA;
+  if (!g_mech_ready[dev]) return MGC_E_NOT_READY;
+  const GasParams p = to_params(gas);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dim == 2) return tu2_mixture_state(gas->nspecies, nnodes, q, t_seed, t1, t2, p, s);
+  if (dim == 3) return tu3_mixture_state(gas->nspecies, nnodes, q, t_seed, t1, t2, p, s);
+  return MGC_E_UNSUPPORTED;
+}
+
+int mgc_euler_rhs(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
+                  const double* t_op, const double* bext, int flux_kind, double* rhs,
+                  int32_t* status, void* stream) {
+  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !rhs || !status) return MGC_E_INVALID;
+  if (flux_kind < 0 || flux_kind > 2) return MGC_E_INVALID;
+  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
+  int rc = ready(mesh, gas);
+  if (rc) return rc;
+  const DGArgs<double> a =
+      make_args(mesh, q, t_op, nullptr, nullptr, rhs, bext, flux_kind, 0, status);
+  return dispatch(1, mesh, gas, a, (cudaStream_t)stream);
+}
+
+int mgc_ns_grad(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
+                const double* t_op, const double* bext, double* grad, int32_t* status,
+                void* stream) {
+  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !grad || !status) return MGC_E_INVALID;
+  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
+  int rc = ready(mesh, gas);
+  if (rc) return rc;
+  const DGArgs<double> a = make_args(mesh, q, t_op, nullptr, nullptr, grad, bext, 0, 0, status);
+  return dispatch(0, mesh, gas, a, (cudaStream_t)stream);
+}
+
+int mgc_ns_rhs(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
+               const double* t_op, const double* t_src, const double* grad,
+               const double* bext, int flux_kind, int add_sources, double* rhs,
+               int32_t* status, void* stream) {
+  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !grad || !rhs || !status) return MGC_E_INVALID;
+  if (flux_kind < 0 || flux_kind > 2) return MGC_E_INVALID;
+  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
+  if (add_sources && (gas->eos_kind != MGC_EOS_MIXTURE || !t_src)) return MGC_E_INVALID;
+  int rc = ready(mesh, gas);
+  if (rc) return rc;
+  const DGArgs<double> a =
+      make_args(mesh, q, t_op, t_src, grad, rhs, bext, flux_kind, add_sources, status);
+  return dispatch(2, mesh, gas, a, (cudaStream_t)stream);
+}
+
+int mgc_rk4_stage(int64_t n, const double* q0, const double* k, double* sum, double* q_out,
+                  float* q_out_lo, int stage, double dt, void* stream) {
+  if (n < 0 || !q0 || !k || !sum || !q_out || stage < 0 || stage > 3) return MGC_E_INVALID;
+  if (n == 0) return MGC_OK;
+  const int nt = 256;
+  int64_t nb = (n + nt - 1) / nt;
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_rk4_stage<float><<<(unsigned)nb, nt, 0, (cudaStream_t)stream>>>(n, q0, k, sum, q_out,
+                                                                    q_out_lo, stage, dt);
+  return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+}
+
+}  // extern "C"

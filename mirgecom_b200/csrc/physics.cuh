@@ -1,0 +1,457 @@
+// Pointwise gas physics for the DG right-hand side kernels.
+//
+// Restates, per node and in registers:
+//   * IdealSingleGas            mirgecom/eos.py:302-537
+//   * PyrometheusMixture        mirgecom/eos.py:540-888 with the fixed-count
+//                               Newton of mirgecom/thermochemistry.py:99-167
+//   * SimpleTransport           mirgecom/transport.py:143-202
+//   * PowerLawTransport         mirgecom/transport.py:205-321
+//   * inviscid flux             mirgecom/inviscid.py:65-102
+//   * viscous flux              mirgecom/viscous.py:72-293
+//   * Rusanov / HLL / central   mirgecom/flux.py:45-177, inviscid.py:105-287
+//   * Arrhenius source terms    mirgecom/eos.py:858-875 (pyrometheus rates,
+//                               concentration floor thermochemistry.py:87-94)
+// Templated on the arithmetic type R (double for the plain path, float for
+// the mixed-precision path).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define MGC_MAX_SPECIES 16
+#define MGC_MAX_REACTIONS 8
+
+namespace mgc {
+
+enum EosKind { EOS_IDEAL = 0, EOS_MIXTURE = 1 };
+enum TransportKind { TR_NONE = 0, TR_SIMPLE = 1, TR_POWERLAW = 2 };
+enum FluxKind { FLUX_RUSANOV = 0, FLUX_HLL = 1, FLUX_CENTRAL = 2 };
+
+// Gas model parameters, passed by value to every kernel.
+struct GasParams {
+  int32_t eos_kind;
+  int32_t nspecies;
+  int32_t niter;            // Newton iterations of the mixture temperature
+  int32_t transport_kind;
+  double gamma, gas_const;  // ideal gas
+  double mu, mu_b, kappa;   // simple transport
+  double pl_alpha, pl_beta, pl_sigma, pl_n;   // power-law transport
+  int32_t use_lewis;
+  int32_t pad_;
+  double diff[MGC_MAX_SPECIES];
+  double lewis[MGC_MAX_SPECIES];
+  double zero_level;        // concentration floor
+};
+
+// Mechanism tables (SI units), uploaded once.
+struct Mechanism {
+  int32_t nspecies, nreactions;
+  double mw[MGC_MAX_SPECIES];
+  double inv_mw[MGC_MAX_SPECIES];
+  double t_mid[MGC_MAX_SPECIES];
+  double a_lo[MGC_MAX_SPECIES][7];
+  double a_hi[MGC_MAX_SPECIES][7];
+  double ord_f[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
+  double nu_p[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
+  double nu_net[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
+  double dnu[MGC_MAX_REACTIONS];
+  double log_a[MGC_MAX_REACTIONS];
+  double beta[MGC_MAX_REACTIONS];
+  double t_act[MGC_MAX_REACTIONS];
+  int32_t reversible[MGC_MAX_REACTIONS];
+};
+
+// one copy per translation unit, filled by mgc_set_mechanism()
+static __constant__ Mechanism c_mech;
+
+constexpr double kGasConstant = 8314.46261815324;
+constexpr double kOneAtm = 101325.0;
+
+// status bits written by kernels (never trapped)
+enum StatusBits {
+  ST_NAN = 1,
+  ST_BAD_INDEX = 2,
+  ST_NEWTON_MISS = 4,
+  ST_NONPOSITIVE = 8,
+};
+
+template <class R> __device__ __forceinline__ R rsqrt_(R x);
+template <> __device__ __forceinline__ double rsqrt_<double>(double x) { return 1.0 / sqrt(x); }
+template <> __device__ __forceinline__ float rsqrt_<float>(float x) { return rsqrtf(x); }
+
+// {{{ NASA-7 thermochemistry
+
+// a[k] for species s at temperature t (high range when t > t_mid)
+template <class R>
+__device__ __forceinline__ R nasa_coef(int s, int k, R t) {
+  return (R)((t > (R)c_mech.t_mid[s]) ? c_mech.a_hi[s][k] : c_mech.a_lo[s][k]);
+}
+
+template <class R>
+__device__ __forceinline__ R species_cp_r(int s, R t) {
+  const R a0 = nasa_coef<R>(s, 0, t), a1 = nasa_coef<R>(s, 1, t),
+          a2 = nasa_coef<R>(s, 2, t), a3 = nasa_coef<R>(s, 3, t),
+          a4 = nasa_coef<R>(s, 4, t);
+  return a0 + a1 * t + a2 * t * t + a3 * t * t * t + a4 * t * t * t * t;
+}
+
+template <class R>
+__device__ __forceinline__ R species_h_rt(int s, R t) {
+  const R a0 = nasa_coef<R>(s, 0, t), a1 = nasa_coef<R>(s, 1, t),
+          a2 = nasa_coef<R>(s, 2, t), a3 = nasa_coef<R>(s, 3, t),
+          a4 = nasa_coef<R>(s, 4, t), a5 = nasa_coef<R>(s, 5, t);
+  return a0 + a1 / (R)2 * t + a2 / (R)3 * t * t + a3 / (R)4 * t * t * t +
+         a4 / (R)5 * t * t * t * t + a5 / t;
+}
+
+template <class R>
+__device__ __forceinline__ R species_s_r(int s, R t) {
+  const R a0 = nasa_coef<R>(s, 0, t), a1 = nasa_coef<R>(s, 1, t),
+          a2 = nasa_coef<R>(s, 2, t), a3 = nasa_coef<R>(s, 3, t),
+          a4 = nasa_coef<R>(s, 4, t), a6 = nasa_coef<R>(s, 6, t);
+  return a0 * log(t) + a1 * t + a2 / (R)2 * t * t + a3 / (R)3 * t * t * t +
+         a4 / (R)4 * t * t * t * t + a6;
+}
+
+// mixture e (J/kg) and c_v (J/kg/K) at temperature t
+template <class R, int NS>
+__device__ __forceinline__ void mixture_e_cv(const R* y, R t, R& e, R& cv) {
+  R se = 0, scv = 0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const R yw = y[s] * (R)c_mech.inv_mw[s];
+    se += yw * (species_h_rt<R>(s, t) - (R)1);
+    scv += yw * (species_cp_r<R>(s, t) - (R)1);
+  }
+  e = (R)kGasConstant * t * se;
+  cv = (R)kGasConstant * scv;
+}
+
+template <class R, int NS>
+__device__ __forceinline__ R mixture_gas_const(const R* y) {
+  R s = 0;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) s += y[k] * (R)c_mech.inv_mw[k];
+  return (R)kGasConstant * s;
+}
+
+template <class R, int NS>
+__device__ __forceinline__ R mixture_cp(const R* y, R t) {
+  R s = 0;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) s += y[k] * species_cp_r<R>(k, t) * (R)c_mech.inv_mw[k];
+  return (R)kGasConstant * s;
+}
+
+// T_{i+1} = T_i + (e - e(T_i)) / c_v(T_i), fixed count
+template <class R, int NS>
+__device__ __forceinline__ R newton_temperature(R e, R tguess, const R* y, int niter) {
+  R t = tguess;
+  for (int it = 0; it < niter; ++it) {
+    R em, cv;
+    mixture_e_cv<R, NS>(y, t, em, cv);
+    t = t + (e - em) / cv;
+  }
+  return t;
+}
+
+// net molar production rates (kmol/m^3/s)
+template <class R, int NS>
+__device__ __forceinline__ void production_rates(R rho, R t, const R* y, R zero_level,
+                                                 R* omega) {
+  R conc[NS];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    R c = (R)c_mech.inv_mw[k] * rho * y[k];
+    conc[k] = (c < zero_level) ? (R)0 : c;
+    omega[k] = 0;
+  }
+  const R logt = log(t);
+  const R invt = (R)1 / t;
+  for (int i = 0; i < c_mech.nreactions; ++i) {
+    const R kf = exp((R)c_mech.log_a[i] + (R)c_mech.beta[i] * logt - (R)c_mech.t_act[i] * invt);
+    R rf = kf;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      const R o = (R)c_mech.ord_f[i][k];
+      if (o != (R)0) rf = rf * ((o == (R)1) ? conc[k] : pow(conc[k], o));
+    }
+    R r = rf;
+    if (c_mech.reversible[i]) {
+      R dg = 0;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        const R nu = (R)c_mech.nu_net[i][k];
+        if (nu != (R)0) dg += nu * (species_h_rt<R>(k, t) - species_s_r<R>(k, t));
+      }
+      const R log_kc = -dg + (R)c_mech.dnu[i] * log((R)kOneAtm / ((R)kGasConstant * t));
+      R rr = kf * exp(-log_kc);
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        const R o = (R)c_mech.nu_p[i][k];
+        if (o != (R)0) rr = rr * ((o == (R)1) ? conc[k] : pow(conc[k], o));
+      }
+      r = rf - rr;
+    }
+#pragma unroll
+    for (int k = 0; k < NS; ++k) omega[k] += (R)c_mech.nu_net[i][k] * r;
+  }
+}
+
+// }}}
+
+// {{{ fluid state at one node
+
+template <class R, int DIM, int NS>
+struct NodeState {
+  R rho, rhoe, mom[DIM], rhoy[NS > 0 ? NS : 1];
+  R v[DIM], y[NS > 0 ? NS : 1];
+  R p, t, c, gamma, cv;
+  R h[NS > 0 ? NS : 1];
+  R mu, mub, kappa, d[NS > 0 ? NS : 1];
+};
+
+// Fill the thermodynamic state.  For the ideal gas the temperature is
+// computed from q; for mixtures *t_in* is the converged temperature.
+template <class R, int DIM, int NS>
+__device__ __forceinline__ void make_state(const R* q, R t_in, const GasParams& g,
+                                           NodeState<R, DIM, NS>& s) {
+  s.rho = q[0];
+  s.rhoe = q[1];
+  R ke = 0;
+  const R irho = (R)1 / s.rho;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) {
+    s.mom[i] = q[2 + i];
+    ke += s.mom[i] * s.mom[i];
+  }
+  ke = (R)0.5 * ke / s.rho;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) s.v[i] = s.mom[i] / s.rho;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    s.rhoy[k] = q[2 + DIM + k];
+    s.y[k] = s.rhoy[k] / s.rho;
+  }
+  (void)irho;
+  if (g.eos_kind == EOS_IDEAL) {
+    const R gam = (R)g.gamma;
+    const R eint = s.rhoe - ke;
+    s.p = eint * (gam - (R)1);
+    s.t = (((gam - (R)1) / (R)g.gas_const) * eint) / s.rho;
+    s.c = sqrt(gam / s.rho * s.p);
+    s.gamma = gam;
+    s.cv = (R)g.gas_const / (gam - (R)1);
+  } else {
+    if constexpr (NS > 0) {
+      s.t = t_in;
+      const R rmix = mixture_gas_const<R, NS>(s.y);
+      s.p = s.rho * rmix * s.t;
+      const R cp = mixture_cp<R, NS>(s.y, s.t);
+      s.gamma = cp / (cp - rmix);
+      s.cv = cp - rmix;
+      s.c = sqrt(s.gamma * s.p / s.rho);
+#pragma unroll
+      for (int k = 0; k < NS; ++k)
+        s.h[k] = ((R)kGasConstant * (R)c_mech.inv_mw[k]) * s.t * species_h_rt<R>(k, s.t);
+    }
+  }
+  // transport
+  if (g.transport_kind == TR_SIMPLE) {
+    s.mu = (R)g.mu;
+    s.mub = (R)g.mu_b;
+    s.kappa = (R)g.kappa;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) s.d[k] = (R)g.diff[k];
+  } else if (g.transport_kind == TR_POWERLAW) {
+    s.mu = (R)g.pl_beta * pow(s.t, (R)g.pl_n);
+    s.mub = (R)g.pl_alpha * s.mu;
+    s.kappa = (R)g.pl_sigma * s.mu * s.cv;
+#pragma unroll
+    for (int k = 0; k < NS; ++k)
+      s.d[k] = g.use_lewis ? (R)g.pl_sigma * s.mu / (s.rho * (R)g.lewis[k] * s.gamma)
+                           : (R)g.diff[k];
+  } else {
+    s.mu = s.mub = s.kappa = 0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) s.d[k] = 0;
+  }
+}
+
+// Temperature of a node from q (ideal: closed form; mixture: Newton from seed)
+template <class R, int DIM, int NS>
+__device__ __forceinline__ R node_temperature(const R* q, R seed, const GasParams& g) {
+  R ke = 0;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) ke += q[2 + i] * q[2 + i];
+  ke = (R)0.5 * ke / q[0];
+  if (g.eos_kind == EOS_IDEAL) {
+    const R gam = (R)g.gamma;
+    return (((gam - (R)1) / (R)g.gas_const) * (q[1] - ke)) / q[0];
+  }
+  if constexpr (NS > 0) {
+    R y[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) y[k] = q[2 + DIM + k] / q[0];
+    const R e = (q[1] - ke) / q[0];
+    return newton_temperature<R, NS>(e, seed, y, g.niter);
+  }
+  return seed;
+}
+
+template <class R, int DIM, int NS>
+__device__ __forceinline__ R wavespeed(const NodeState<R, DIM, NS>& s) {
+  R v2 = 0;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) v2 += s.v[i] * s.v[i];
+  return sqrt(v2) + s.c;
+}
+
+// }}}
+
+// {{{ fluxes
+
+// inviscid flux dotted with n: F_I(q) . n   (mirgecom/inviscid.py:65-102)
+template <class R, int DIM, int NS>
+__device__ __forceinline__ void inviscid_flux_n(const NodeState<R, DIM, NS>& s, const R* n,
+                                                R* fn) {
+  R vn = 0, mn = 0;
+#pragma unroll
+  for (int j = 0; j < DIM; ++j) {
+    vn += s.v[j] * n[j];
+    mn += s.mom[j] * n[j];
+  }
+  fn[0] = mn;
+  fn[1] = vn * (s.rhoe + s.p);
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) {
+    R a = 0;
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) a += (s.rho * s.v[i] * s.v[j] + ((i == j) ? s.p : (R)0)) * n[j];
+    fn[2 + i] = a;
+  }
+#pragma unroll
+  for (int k = 0; k < NS; ++k) fn[2 + DIM + k] = vn * s.rhoy[k];
+}
+
+// full inviscid flux F_I[c][j]
+template <class R, int DIM, int NS>
+__device__ __forceinline__ void inviscid_flux(const NodeState<R, DIM, NS>& s,
+                                              R (*f)[DIM]) {
+#pragma unroll
+  for (int j = 0; j < DIM; ++j) {
+    f[0][j] = s.mom[j];
+    f[1][j] = s.v[j] * (s.rhoe + s.p);
+#pragma unroll
+    for (int i = 0; i < DIM; ++i)
+      f[2 + i][j] = s.rho * s.v[i] * s.v[j] + ((i == j) ? s.p : (R)0);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) f[2 + DIM + k][j] = s.v[j] * s.rhoy[k];
+  }
+}
+
+// viscous flux F_V[c][j] from gradients gq[c][j] (c < NC) and gt[j]
+template <class R, int DIM, int NS, bool MIXTURE>
+__device__ __forceinline__ void viscous_flux(const NodeState<R, DIM, NS>& s,
+                                             const R (*gq)[DIM], const R* gt,
+                                             R (*f)[DIM]) {
+  const R irho = (R)1 / s.rho;
+  R gv[DIM][DIM];
+  R divv = 0;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) {
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) gv[i][j] = (gq[2 + i][j] - s.v[i] * gq[0][j]) / s.rho;
+    divv += gv[i][i];
+  }
+  (void)irho;
+  R tau[DIM][DIM];
+  const R lam = (s.mub - (R)2 * s.mu / (R)3) * divv;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i)
+#pragma unroll
+    for (int j = 0; j < DIM; ++j)
+      tau[i][j] = s.mu * (gv[i][j] + gv[j][i]) + ((i == j) ? lam : (R)0);
+#pragma unroll
+  for (int j = 0; j < DIM; ++j) {
+    f[0][j] = 0;
+    R ef = 0;
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) ef += tau[j][i] * s.v[i];
+    ef = ef + s.kappa * gt[j];
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) f[2 + i][j] = tau[i][j];
+    f[1][j] = ef;
+  }
+  if constexpr (NS > 0) {
+    R gy[NS][DIM];
+#pragma unroll
+    for (int k = 0; k < NS; ++k)
+#pragma unroll
+      for (int j = 0; j < DIM; ++j) gy[k][j] = (gq[2 + DIM + k][j] - s.y[k] * gq[0][j]) / s.rho;
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) {
+      if constexpr (MIXTURE) {
+        R sum_dgy = 0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) sum_dgy += s.d[k] * gy[k][j];
+        R qd = 0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          const R jk = -s.rho * (s.d[k] * gy[k][j] - s.y[k] * sum_dgy);
+          qd += s.h[k] * jk;
+          f[2 + DIM + k][j] = -jk;
+        }
+        f[1][j] = f[1][j] - qd;
+      } else {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) f[2 + DIM + k][j] = s.rho * (s.d[k] * gy[k][j]);
+      }
+    }
+  }
+}
+
+// numerical inviscid flux F*_I . n between interior (m) and exterior (p)
+template <class R, int DIM, int NS>
+__device__ __forceinline__ void inviscid_num_flux(const NodeState<R, DIM, NS>& sm,
+                                                  const NodeState<R, DIM, NS>& sp,
+                                                  const R* qm, const R* qp, const R* n,
+                                                  int kind, R* out) {
+  constexpr int NC = DIM + 2 + NS;
+  R fm[NC], fp[NC];
+  inviscid_flux_n<R, DIM, NS>(sm, n, fm);
+  inviscid_flux_n<R, DIM, NS>(sp, n, fp);
+  if (kind == FLUX_HLL) {
+    R u_int = 0, u_ext = 0;
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) {
+      u_int += sm.v[j] * n[j];
+      u_ext += sp.v[j] * n[j];
+    }
+    const R p_star = ((R)0.5 * (sm.p + sp.p) +
+                      ((R)1 / (R)8) * (u_int - u_ext) * (sm.rho + sp.rho) * (sm.c + sp.c));
+    const R q_int = (R)1 + (sm.gamma + (R)1) / ((R)2 * sm.gamma) * (p_star / sm.p - (R)1);
+    const R q_ext = (R)1 + (sp.gamma + (R)1) / ((R)2 * sp.gamma) * (p_star / sp.p - (R)1);
+    const R q_int_rt = sqrt((p_star > sm.p) ? q_int : (R)1);
+    const R q_ext_rt = sqrt((p_star > sp.p) ? q_ext : (R)1);
+    const R s_minus = u_int - sm.c * q_int_rt;
+    const R s_plus = u_ext + sp.c * q_ext_rt;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      R f = (s_plus * fm[c] - s_minus * fp[c] + s_plus * s_minus * (qp[c] - qm[c])) /
+            (s_plus - s_minus);
+      if (s_minus >= (R)0) f = fm[c];
+      if (s_plus <= (R)0) f = fp[c];
+      out[c] = f;
+    }
+  } else {
+    const R lam = (kind == FLUX_RUSANOV)
+                      ? fmax(wavespeed<R, DIM, NS>(sm), wavespeed<R, DIM, NS>(sp))
+                      : (R)0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) out[c] = (fm[c] + fp[c] + lam * (qm[c] - qp[c])) / (R)2;
+  }
+}
+
+// }}}
+
+}  // namespace mgc

@@ -1,0 +1,27 @@
+// Kernel instantiations for 3-D simplices (float64 plain path).
+#include "dg_dispatch.cuh"
+
+namespace mgc {
+
+int tu3_upload_refops(int dim, int order, const double* p64, const float* p32, const int* fn) {
+  return upload_refops_local(dim, order, p64, p32, fn);
+}
+
+int tu3_upload_mechanism(const Mechanism* m) { return upload_mechanism_local(m); }
+
+int tu3_dispatch(int op, int order, int ns, bool mix, const DGArgs<double>& a,
+                    const GasParams& g, cudaStream_t s) {
+  switch (order) {
+    case 1: return dispatch_order<double, 3, 1>(op, ns, mix, a, g, s);
+    case 2: return dispatch_order<double, 3, 2>(op, ns, mix, a, g, s);
+    case 3: return dispatch_order<double, 3, 3>(op, ns, mix, a, g, s);
+    default: return MGC_E_UNSUPPORTED;
+  }
+}
+
+int tu3_mixture_state(int ns, int64_t nnodes, const double* q, const double* tseed,
+                         double* t1, double* t2, const GasParams& g, cudaStream_t s) {
+  return mixture_state_dim<double, 3>(ns, nnodes, q, tseed, t1, t2, g, s);
+}
+
+}  // namespace mgc

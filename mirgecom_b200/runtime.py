@@ -1,0 +1,273 @@
+"""Device runtime: uploads, workspaces and the C-ABI launches.
+
+One :class:`DeviceDiscretization` per (Discretization, device) holds the
+uploaded index arrays and geometry, the ``mgc_mesh_t`` descriptor and the
+reusable workspaces (gradients, temperatures, boundary exterior states), so
+that an RHS evaluation allocates nothing after its first call.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from mirgecom_b200 import _lib
+
+_uploaded_refops = set()     # (device index, dim, order)
+_uploaded_mech = {}          # device index -> id(mechanism)
+
+
+def _dev_index(device):
+    return device.index if device.index is not None else torch.cuda.current_device()
+
+
+def ensure_reference_operators(dcoll, device):
+    key = (_dev_index(device), dcoll.dim, dcoll.order)
+    if key in _uploaded_refops:
+        return
+    r = dcoll.refel
+    if r.kind != "simplex":
+        raise NotImplementedError("device kernels cover simplicial elements")
+    lib = _lib.load()
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
+            (r.weak, r.lift, r.ref_face_normals, r.face_scale_ref)]
+    fn = np.ascontiguousarray(r.face_nodes, dtype=np.int32)
+    with torch.cuda.device(device):
+        _lib.check(lib.mgc_upload_reference_operators(
+            dcoll.dim, dcoll.order, *[_lib.ptr(a) for a in arrs], _lib.ptr(fn)),
+            "mgc_upload_reference_operators")
+    _uploaded_refops.add(key)
+
+
+def ensure_mechanism(eos, device):
+    idx = _dev_index(device)
+    if _uploaded_mech.get(idx) is eos.mechanism:
+        return
+    lib = _lib.load()
+    ms = eos.mechanism_struct()
+    with torch.cuda.device(device):
+        _lib.check(lib.mgc_set_mechanism(C.byref(ms)), "mgc_set_mechanism")
+    _uploaded_mech[idx] = eos.mechanism
+
+
+class DeviceDiscretization:
+    def __init__(self, dcoll, device):
+        self.dcoll = dcoll
+        self.device = device
+        c = dcoll.connectivity
+        g = dcoll.geometry
+        self.rx = torch.from_numpy(np.ascontiguousarray(g.rx)).to(device)
+        self.conn = torch.from_numpy(np.ascontiguousarray(c.conn, dtype=np.int32)).to(device)
+        self.perm = torch.from_numpy(np.ascontiguousarray(c.perm, dtype=np.uint8)).to(device)
+        nbf = len(c.bface_elem)
+        self.nbf = nbf
+        self.bface_elem = torch.from_numpy(c.bface_elem).to(device)
+        self.bface_nodes = torch.from_numpy(
+            dcoll.refel.face_nodes[c.bface_face].astype(np.int64)).to(device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        self._bkind_cache = {}
+        self._work = {}
+        self.mesh = _lib.MeshStruct()
+        self.mesh.dim = dcoll.dim
+        self.mesh.order = dcoll.order
+        self.mesh.nelem = dcoll.nelements
+        self.mesh.nbf = nbf
+        self.mesh.nperm = len(c.perm)
+        self.mesh.rx = self.rx.data_ptr()
+        self.mesh.conn = self.conn.data_ptr()
+        self.mesh.perm = self.perm.data_ptr()
+        self.mesh.bkind = None
+
+    def workspace(self, name, shape, dtype=torch.float64):
+        t = self._work.get(name)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            t = torch.empty(shape, dtype=dtype, device=self.device)
+            self._work[name] = t
+        return t
+
+    def bkind_for(self, boundaries):
+        """int8 [nbf] boundary kinds for this *boundaries* dict."""
+        key = tuple(sorted((str(tag), type(b).__name__) for tag, b in boundaries.items()))
+        if key not in self._bkind_cache:
+            kinds = np.zeros(max(self.nbf, 1), dtype=np.int8)
+            covered = np.zeros(self.nbf, dtype=bool)
+            for tag, bdry in boundaries.items():
+                mask = self.dcoll.boundary_face_mask(tag)
+                kinds[:self.nbf][mask] = bdry.device_kind
+                covered |= mask
+            if self.nbf and not covered.all():
+                raise ValueError("some boundary faces have no boundary condition")
+            self._bkind_cache[key] = torch.from_numpy(kinds).to(self.device)
+        return self._bkind_cache[key]
+
+
+def device_discretization(dcoll, device) -> DeviceDiscretization:
+    cache = dcoll.__dict__.setdefault("_device_cache", {})
+    key = _dev_index(device)
+    if key not in cache:
+        cache[key] = DeviceDiscretization(dcoll, device)
+    ensure_reference_operators(dcoll, device)
+    return cache[key]
+
+
+def _gas_struct(gas_model, nspecies, device):
+    if gas_model.eos.is_mixture:
+        ensure_mechanism(gas_model.eos, device)
+    return gas_model.to_struct(nspecies)
+
+
+def mixture_temperature(cv, gas_model, tseed):
+    """Launch the Newton temperature kernel: returns (T1, T2)."""
+    q = cv.q
+    _lib.require_cuda(q)
+    lib = _lib.load()
+    gs = _gas_struct(gas_model, cv.nspecies, q.device)
+    n = q[0].numel()
+    t1 = torch.empty_like(q[0])
+    t2 = torch.empty_like(q[0])
+    tseed = tseed.to(dtype=q.dtype).contiguous()
+    with torch.cuda.device(q.device):
+        _lib.check(lib.mgc_mixture_temperature(
+            cv.dim, C.byref(gs), n, _lib.ptr(q), _lib.ptr(tseed), _lib.ptr(t1),
+            _lib.ptr(t2), _lib.stream_handle()), "mgc_mixture_temperature")
+    return t1, t2
+
+
+def boundary_exterior(dd, state, gas_model, boundaries, time):
+    """[Nc+1, nbf, Nfp] exterior states of the prescribed boundaries, or None."""
+    from mirgecom_b200.boundary import PrescribedFluidBoundary
+    if not any(isinstance(b, PrescribedFluidBoundary) for b in boundaries.values()):
+        return None
+    dcoll = dd.dcoll
+    q = state.cv.q
+    nc = q.shape[0]
+    nfp = dcoll.nface_nodes
+    bext = dd.workspace("bext", (nc + 1, dd.nbf, nfp), q.dtype)
+    be = dd.bface_elem[:, None]
+    qm = q[:, be, dd.bface_nodes]                          # [Nc, nbf, Nfp]
+    from mirgecom_b200.fluid import ConservedVars
+    from mirgecom_b200.gas_model import FluidState
+    tm = None
+    if state.is_mixture:
+        tm = state.temperature[be, dd.bface_nodes]
+    for tag, bdry in boundaries.items():
+        if not isinstance(bdry, PrescribedFluidBoundary):
+            continue
+        mask = torch.from_numpy(dcoll.boundary_face_mask(tag)).to(q.device)
+        sm = FluidState(ConservedVars(qm[:, mask], state.dim), gas_model,
+                        temperature=None if tm is None else tm[mask])
+        ext = bdry.exterior_state(dcoll, tag, gas_model, sm, time,
+                                  nodes=dcoll.boundary_nodes(tag, q.device))
+        bext[:nc, mask] = ext.cv.q.to(q.dtype)
+        if state.is_mixture:
+            bext[nc, mask] = ext.temperature.to(q.dtype)
+    return bext
+
+
+def _operator_temperature(state):
+    if not state.is_mixture:
+        return None
+    if state.operator_temperature is None:
+        # the operator states re-solve from the state temperature
+        _, t2 = mixture_temperature(state.cv, state.gas_model, state.temperature)
+        state.operator_temperature = t2
+    return state.operator_temperature.contiguous()
+
+
+def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
+    q = state.cv.q
+    _lib.require_cuda(q)
+    q = q.contiguous()
+    lib = _lib.load()
+    dd = device_discretization(dcoll, q.device)
+    gs = _gas_struct(gas_model, state.cv.nspecies, q.device)
+    bkind = dd.bkind_for(boundaries)
+    dd.mesh.bkind = bkind.data_ptr()
+    bext = boundary_exterior(dd, state, gas_model, boundaries, time)
+    t_op = _operator_temperature(state)
+    rhs = torch.empty_like(q)
+    with torch.cuda.device(q.device):
+        _lib.check(lib.mgc_euler_rhs(
+            C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(bext),
+            flux_kind, _lib.ptr(rhs), _lib.ptr(dd.status), _lib.stream_handle()),
+            "mgc_euler_rhs")
+    return rhs
+
+
+def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
+           source_temperature=None, grad_out=None, events=None):
+    """Gradient + divergence passes.  *events* (3 CUDA events) are recorded
+    before the gradient pass, between the passes and after the divergence."""
+    q = state.cv.q
+    _lib.require_cuda(q)
+    q = q.contiguous()
+    lib = _lib.load()
+    dd = device_discretization(dcoll, q.device)
+    nc = q.shape[0]
+    gs = _gas_struct(gas_model, state.cv.nspecies, q.device)
+    bkind = dd.bkind_for(boundaries)
+    dd.mesh.bkind = bkind.data_ptr()
+    bext = boundary_exterior(dd, state, gas_model, boundaries, time)
+    t_op = _operator_temperature(state)
+    grad = grad_out if grad_out is not None else dd.workspace(
+        "grad", (nc + 1, dcoll.dim) + tuple(q.shape[1:]), q.dtype)
+    rhs = torch.empty_like(q)
+    stream = _lib.stream_handle()
+    add_src = source_temperature is not None
+    t_src = source_temperature.contiguous() if add_src else None
+    with torch.cuda.device(q.device):
+        if events:
+            events[0].record()
+        _lib.check(lib.mgc_ns_grad(
+            C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(bext),
+            _lib.ptr(grad), _lib.ptr(dd.status), stream), "mgc_ns_grad")
+        if events:
+            events[1].record()
+        _lib.check(lib.mgc_ns_rhs(
+            C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(t_src),
+            _lib.ptr(grad), _lib.ptr(bext), flux_kind, int(add_src), _lib.ptr(rhs),
+            _lib.ptr(dd.status), stream), "mgc_ns_rhs")
+        if events:
+            events[2].record()
+    return rhs, grad
+
+
+def read_status(dcoll, device=None, reset=True):
+    """Device status bits accumulated by the kernels (synchronises)."""
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    dd = device_discretization(dcoll, device)
+    val = int(dd.status.item())
+    if reset:
+        dd.status.zero_()
+    return val
+
+
+def rk4_stage(q0, k, acc, qout, stage, dt, qout_lo=None):
+    lib = _lib.load()
+    n = q0.numel()
+    _lib.check(lib.mgc_rk4_stage(n, _lib.ptr(q0), _lib.ptr(k), _lib.ptr(acc), _lib.ptr(qout),
+                                 _lib.ptr(qout_lo), stage, float(dt), _lib.stream_handle()),
+               "mgc_rk4_stage")
+
+
+def ns_gradients(dcoll, state, gas_model, boundaries, time):
+    """Gradient pass only: [Nc+1, dim, E, Np] (workspace tensor)."""
+    q = state.cv.q
+    _lib.require_cuda(q)
+    q = q.contiguous()
+    lib = _lib.load()
+    dd = device_discretization(dcoll, q.device)
+    nc = q.shape[0]
+    gs = _gas_struct(gas_model, state.cv.nspecies, q.device)
+    bkind = dd.bkind_for(boundaries)
+    dd.mesh.bkind = bkind.data_ptr()
+    bext = boundary_exterior(dd, state, gas_model, boundaries, time)
+    t_op = _operator_temperature(state)
+    grad = dd.workspace("grad", (nc + 1, dcoll.dim) + tuple(q.shape[1:]), q.dtype)
+    with torch.cuda.device(q.device):
+        _lib.check(lib.mgc_ns_grad(
+            C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(bext),
+            _lib.ptr(grad), _lib.ptr(dd.status), _lib.stream_handle()), "mgc_ns_grad")
+    return grad

@@ -1,0 +1,78 @@
+"""Matched product / oracle set-ups for the parity tests."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from mirgecom_b200.discretization import Discretization
+from mirgecom_b200.mesh import generate_box_mesh
+from oracle import dg as odg
+from oracle import physics as oph
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def field_rel_l2(a, b):
+    """Largest per-field relative L2 error (fields along axis 0)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    tot = np.linalg.norm(b.ravel())
+    errs = []
+    for c in range(b.shape[0]):
+        den = max(np.linalg.norm(b[c].ravel()), 1e-6 * tot, 1e-300)
+        errs.append(np.linalg.norm((a[c] - b[c]).ravel()) / den)
+    return float(max(errs))
+
+
+def make_disc(kind, dim, n, order, lo, hi, periodic):
+    mesh = generate_box_mesh(lo, hi, (n,) * dim, kind=kind, periodic=(periodic,) * dim
+                             if isinstance(periodic, bool) else periodic)
+    d = Discretization(mesh, order)
+    od = odg.OracleDisc(mesh, d.refel)
+    return d, od
+
+
+def vortex_np(x, t=0.0, beta=5.0, center=(5.0, 0.0), vel=(1.0, 0.0), gamma=1.4):
+    xr = x[0] - center[0] - t * vel[0]
+    yr = x[1] - center[1] - t * vel[1]
+    r = np.sqrt(xr ** 2 + yr ** 2)
+    ex = beta * np.exp(1 - r ** 2)
+    u = vel[0] - ex * yr / (2 * np.pi)
+    v = vel[1] + ex * xr / (2 * np.pi)
+    rho = (1 - (gamma - 1) / (16 * gamma * np.pi ** 2) * ex ** 2) ** (1 / (gamma - 1))
+    p = rho ** gamma
+    return np.array([rho, p / (gamma - 1) + rho / 2 * (u ** 2 + v ** 2), rho * u, rho * v])
+
+
+def tgv_np(x, gamma=1.4, mach=0.1):
+    u = np.sin(x[0]) * np.cos(x[1]) * np.cos(x[2])
+    v = -np.cos(x[0]) * np.sin(x[1]) * np.cos(x[2])
+    w = np.zeros_like(u)
+    p0 = 1.0 / (gamma * mach ** 2)
+    p = p0 + 1.0 / 16 * (np.cos(2 * x[0]) + np.cos(2 * x[1])) * (np.cos(2 * x[2]) + 2)
+    rho = np.ones_like(u)
+    return np.array([rho, p / (gamma - 1) + 0.5 * (u * u + v * v), u, v, w])
+
+
+def perturbed_state_np(x, dim, nspecies, seed=0):
+    """Smooth non-uniform ideal-gas state with passive species."""
+    rng = np.random.default_rng(seed)
+    k = rng.uniform(0.5, 1.5, size=(6, dim))
+    ph = rng.uniform(0, 2 * np.pi, size=6)
+    def f(i):
+        return np.cos(sum(k[i, d] * x[d] for d in range(dim)) + ph[i])
+    rho = 1.0 + 0.2 * f(0)
+    vel = [0.3 * f(1 + (j % 3)) for j in range(dim)]
+    p = 1.0 + 0.1 * f(4)
+    e = p / 0.4 + 0.5 * rho * sum(v * v for v in vel)
+    q = [rho, e] + [rho * v for v in vel]
+    for s in range(nspecies):
+        q.append(rho * (0.1 + 0.05 * (s + 1) * (1 + f(5))))
+    return np.array(q)
