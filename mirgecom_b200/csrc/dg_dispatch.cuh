@@ -42,32 +42,26 @@ inline int prepare_kernel(Kern kern, size_t smem) {
   return MGC_OK;
 }
 
-template <class R, int DIM, int ORDER, int NS, bool MIX>
+template <int DIM, int ORDER, int NS, bool MIX>
 struct Launch {
-  using C = Cfg<R, DIM, ORDER, NS, MIX>;
-  static size_t smem_grad(int nperm) {
-    return (size_t)C::EPB_GRAD * C::BYTES_GRAD + C::NFN * sizeof(int) + (size_t)nperm * C::NFP + 16;
-  }
-  static size_t smem_rhs(int nperm) {
-    return (size_t)C::EPB_RHS * C::BYTES_RHS + C::NFN * sizeof(int) + (size_t)nperm * C::NFP + 16;
-  }
-  static int grad(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
-    const size_t smem = smem_grad(a.nperm);
-    auto kern = k_grad<R, DIM, ORDER, NS, MIX>;
+  using C = Cfg<DIM, ORDER, NS, MIX>;
+  static int grad(const DGArgs<double>& a, const GasParams& g, cudaStream_t s) {
+    const size_t smem = C::smem_grad(a.nperm);
+    auto kern = k_grad<DIM, ORDER, NS, MIX>;
     int rc = prepare_kernel(kern, smem);
     if (rc) return rc;
     const int nblk = (a.nelem + C::EPB_GRAD - 1) / C::EPB_GRAD;
-    kern<<<nblk, C::NT_GRAD, smem, s>>>(a, g);
+    kern<<<nblk, C::NT, smem, s>>>(a, g);
     return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
   }
   template <bool VISC>
-  static int rhs(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
-    const size_t smem = smem_rhs(a.nperm);
-    auto kern = k_rhs<R, DIM, ORDER, NS, MIX, VISC>;
+  static int rhs(const DGArgs<double>& a, const GasParams& g, cudaStream_t s) {
+    const size_t smem = C::smem_rhs(a.nperm);
+    auto kern = k_rhs<DIM, ORDER, NS, MIX, VISC>;
     int rc = prepare_kernel(kern, smem);
     if (rc) return rc;
     const int nblk = (a.nelem + C::EPB_RHS - 1) / C::EPB_RHS;
-    kern<<<nblk, C::NT_RHS, smem, s>>>(a, g);
+    kern<<<nblk, C::NT, smem, s>>>(a, g);
     return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
   }
 };
@@ -78,7 +72,7 @@ inline int dispatch_order(int op, int ns, bool mix, const DGArgs<R>& a, const Ga
                           cudaStream_t s) {
 #define MGC_CASE(NSV, MIXV)                                              \
   if (ns == NSV && mix == MIXV) {                                        \
-    using L = Launch<R, DIM, ORDER, NSV, MIXV>;                          \
+    using L = Launch<DIM, ORDER, NSV, MIXV>;                             \
     if (op == 0) return L::grad(a, g, s);                                \
     if (op == 1) return L::template rhs<false>(a, g, s);                 \
     return L::template rhs<true>(a, g, s);                               \

@@ -60,27 +60,71 @@ __host__ __device__ constexpr int imin(int a, int b) { return a < b ? a : b; }
 __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
-template <class R, int DIM, int ORDER, int NS, bool MIX>
+// Padded row stride (in doubles) of a shared-memory operand matrix read as
+// m8n8k4 f64 MMA fragments: rows hold K entries (rounded to the k-step 4),
+// and stride = 4 (mod 16) keeps each half-warp's 16 loads on distinct banks.
+__host__ __device__ constexpr int mma_stride(int k) {
+  return round_up(k, 4) + ((4 - round_up(k, 4) % 16) + 16) % 16;
+}
+
+template <int DIM, int ORDER, int NS, bool MIX>
 struct Cfg {
   using S = Simplex<DIM, ORDER>;
   static constexpr int NP = S::NP, NF = S::NF, NFP = S::NFP;
   static constexpr int NFN = NF * NFP;
   static constexpr int NC = DIM + 2 + NS;
   static constexpr int NU = NC + 1;      // conserved fields + temperature
-  static constexpr int SMEM_BUDGET = 96 * 1024;
-  // per-element shared bytes
+  static constexpr int MP = round_up(NP, 8);           // output rows, padded
+  static constexpr int MT = MP / 8;                    // m-tiles
+  static constexpr int NT = 256;                       // threads per CTA
+  // two resident CTAs per SM (<= 128 registers) unless the species make the
+  // pointwise flux state too large for that
+  static constexpr int MINB = (NC <= 7) ? 2 : 1;
+  static constexpr int SMEM_BUDGET = 112 * 1024;
   static constexpr int GEO = DIM * DIM + NF * (DIM + 1);
-  static constexpr int BYTES_GRAD = (NU * NP + NU * NFN + GEO) * (int)sizeof(R);
-  static constexpr int BYTES_RHS =
-      (NC * NP + (MIX ? 2 * NP : 0) + DIM * NC * NP + NC * NFN + NS * NP + GEO) * (int)sizeof(R);
-  static constexpr int EPB_GRAD = imax(1, imin(imin(128 / NU, 32), SMEM_BUDGET / BYTES_GRAD));
-  static constexpr int EPB_RHS = imax(1, imin(imin(128 / NC, 32), SMEM_BUDGET / BYTES_RHS));
-  // 256 threads leave up to 255 registers per thread for the register-resident
-  // contraction operands; the pointwise phases stride over the tile
-  static constexpr int NT_GRAD = 256;
-  static constexpr int NT_RHS = 256;
-  static constexpr int PERM_MAX = 256 * NFP;
+
+  // gradient kernel operands: U [col][KU], face values [col][KS] with
+  // col = field * EPB + element; matrices AW [DIM][MP][KU], AL [NF][MP][KL]
+  static constexpr int NFP4 = round_up(NFP, 4);
+  static constexpr int KU = mma_stride(NP);
+  static constexpr int KS = mma_stride(NF * NFP4);
+  static constexpr int KL = mma_stride(NFP4);
+  static constexpr int G_MAT = DIM * MP * KU + NF * MP * KL;
+  static constexpr int G_PER_ELEM = NU * (KU + KS) + GEO;
+  static constexpr int EPB_G_RAW = (SMEM_BUDGET / 8 - G_MAT - 512) / G_PER_ELEM;
+  static constexpr int EPB_GRAD = imax(8, imin(32, EPB_G_RAW / 8 * 8));
+  static constexpr int NCOL_G = round_up(NU * EPB_GRAD, 8);
+
+  // rhs kernel operands: B [col][KB] = [G_0 .. G_{DIM-1} | S] per column,
+  // A [MP][KB] = [-W_0 .. -W_{DIM-1} | LIFT]
+  static constexpr int KR = DIM * NP + NFN;
+  static constexpr int KB = mma_stride(KR);
+  static constexpr int R_MAT = MP * KB;
+  static constexpr int R_PER_ELEM = NC * KB + NC * NP + (MIX ? 2 * NP : 0) + NS * NP + GEO;
+  static constexpr int EPB_R_RAW = (SMEM_BUDGET / 8 - R_MAT - 512) / R_PER_ELEM;
+  static constexpr int EPB_RHS = imax(4, imin(32, EPB_R_RAW >= 8 ? EPB_R_RAW / 8 * 8
+                                                                 : EPB_R_RAW / 4 * 4));
+  static constexpr int NCOL_R = round_up(NC * EPB_RHS, 8);
+
+  static size_t smem_grad(int nperm) {
+    return (size_t)(G_MAT + NCOL_G * (KU + KS) + EPB_GRAD * GEO) * 8 + NFN * 4 +
+           (size_t)nperm * NFP + 64;
+  }
+  static size_t smem_rhs(int nperm) {
+    return (size_t)(R_MAT + NCOL_R * KB + EPB_RHS * (NC * NP + (MIX ? 2 * NP : 0) + NS * NP + GEO)) * 8 +
+           NFN * 4 + (size_t)nperm * NFP + 64;
+  }
 };
+
+// D(8x8) += A(8x4) * B(4x8), float64 tensor-core MMA.  Fragments:
+//   A: lane holds A[lane/4][lane%4];  B: lane holds B[lane%4][lane/4];
+//   D: lane holds D[lane/4][2*(lane%4) + {0,1}].
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
 
 // Per-element geometry: rx copy, unit normals and face factors derived from rx
 // (n dS = J rx^T N dS_ref;  fscale = |rx^T N| * face_scale_ref).
@@ -135,19 +179,21 @@ __global__ void __launch_bounds__(256) k_mixture_state(int64_t nnodes, const R* 
 
 // {{{ gradient kernel
 
-template <class R, int DIM, int ORDER, int NS, bool MIX>
-__global__ void __launch_bounds__((Cfg<R, DIM, ORDER, NS, MIX>::NT_GRAD))
-    k_grad(DGArgs<R> a, GasParams g) {
-  using C = Cfg<R, DIM, ORDER, NS, MIX>;
+template <int DIM, int ORDER, int NS, bool MIX>
+__global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_grad(DGArgs<double> a, GasParams g) {
+  using C = Cfg<DIM, ORDER, NS, MIX>;
   using S = Simplex<DIM, ORDER>;
   constexpr int NP = C::NP, NF = C::NF, NFP = C::NFP, NFN = C::NFN, NC = C::NC, NU = C::NU;
-  constexpr int EPB = C::EPB_GRAD;
+  constexpr int EPB = C::EPB_GRAD, MP = C::MP, MT = C::MT;
+  constexpr int KU = C::KU, KS = C::KS, KL = C::KL, NFP4 = C::NFP4, NCOL = C::NCOL_G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* u_s = reinterpret_cast<R*>(smem_raw);                 // [NU][EPB][NP]
-  R* f_s = u_s + NU * EPB * NP;                            // [NU][EPB][NFN]
-  R* rx_s = f_s + NU * EPB * NFN;                          // [EPB][DIM][DIM]
-  R* nrm_s = rx_s + EPB * DIM * DIM;                       // [EPB][NF][DIM]
-  R* fs_s = nrm_s + EPB * NF * DIM;                        // [EPB][NF]
+  double* aw = reinterpret_cast<double*>(smem_raw);        // [DIM][MP][KU]
+  double* al = aw + DIM * MP * KU;                         // [NF][MP][KL]
+  double* bu = al + NF * MP * KL;                          // [NCOL][KU]
+  double* bs = bu + NCOL * KU;                              // [NCOL][KS]
+  double* rx_s = bs + NCOL * KS;                           // [EPB][DIM][DIM]
+  double* nrm_s = rx_s + EPB * DIM * DIM;                  // [EPB][NF][DIM]
+  double* fs_s = nrm_s + EPB * NF * DIM;                   // [EPB][NF]
   int* fn_s = reinterpret_cast<int*>(fs_s + EPB * NF);     // [NF*NFP]
   uint8_t* perm_s = reinterpret_cast<uint8_t*>(fn_s + NFN);
 
@@ -156,34 +202,51 @@ __global__ void __launch_bounds__((Cfg<R, DIM, ORDER, NS, MIX>::NT_GRAD))
   const int ne = imin(EPB, E - e0);
   const int64_t EN = (int64_t)E * NP;
 
+  // reference operators (zero padded) and zeroed operand tiles
+  for (int i = threadIdx.x; i < DIM * MP * KU; i += blockDim.x) {
+    const int r = i / (MP * KU), row = (i / KU) % MP, k = i % KU;
+    aw[i] = (row < NP && k < NP) ? c_ref64[S::OFF_W + (r * NP + row) * NP + k] : 0.0;
+  }
+  for (int i = threadIdx.x; i < NF * MP * KL; i += blockDim.x) {
+    const int f = i / (MP * KL), row = (i / KL) % MP, m = i % KL;
+    al[i] = (row < NP && m < NFP) ? c_ref64[S::OFF_LIFT + row * NFN + f * NFP + m] : 0.0;
+  }
+  for (int i = threadIdx.x; i < NCOL * (KU + KS); i += blockDim.x) bu[i] = 0.0;
   for (int i = threadIdx.x; i < NFN; i += blockDim.x) fn_s[i] = c_face_nodes<DIM, ORDER>(i);
   for (int i = threadIdx.x; i < a.nperm * NFP; i += blockDim.x) perm_s[i] = a.perm[i];
-  // phase 1: tile load
+  load_geometry<double, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);   // syncs once
+  __syncthreads();
+
+  // phase 1: conserved fields (and temperature) of the tile into U
   for (int c = 0; c < NC; ++c)
-    for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x)
-      u_s[(c * EPB) * NP + idx] = a.q[c * EN + (int64_t)e0 * NP + idx];
+    for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
+      const int e = idx / NP, k = idx % NP;
+      bu[(c * EPB + e) * KU + k] = a.q[c * EN + (int64_t)e0 * NP + idx];
+    }
   if (MIX)
-    for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x)
-      u_s[(NC * EPB) * NP + idx] = a.t_op[(int64_t)e0 * NP + idx];
-  load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
+    for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
+      const int e = idx / NP, k = idx % NP;
+      bu[(NC * EPB + e) * KU + k] = a.t_op[(int64_t)e0 * NP + idx];
+    }
   __syncthreads();
   if (!MIX) {
     for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
-      R qq[NC];
+      const int e = idx / NP, k = idx % NP;
+      double qq[NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) qq[c] = u_s[(c * EPB) * NP + idx];
-      u_s[(NC * EPB) * NP + idx] = node_temperature<R, DIM, NS>(qq, (R)0, g);
+      for (int c = 0; c < NC; ++c) qq[c] = bu[(c * EPB + e) * KU + k];
+      bu[(NC * EPB + e) * KU + k] = node_temperature<double, DIM, NS>(qq, 0.0, g);
     }
     __syncthreads();
   }
 
-  // phase 3: face values  fscale * u*   (u* = central / boundary value)
+  // phase 3: face values  fscale * u*   (u* = central average or boundary value)
   for (int idx = threadIdx.x; idx < ne * NFN; idx += blockDim.x) {
     const int e = idx / NFN, fm = idx % NFN, f = fm / NFP, m = fm % NFP;
     const int k = fn_s[fm];
     const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
-    const R fsc = fs_s[e * NF + f];
-    R up[NU];
+    const double fsc = fs_s[e * NF + f];
+    double up[NU];
     bool central = true;
     if (cn >= 0) {
       const int en = cn >> 8, pr = cn & 255;
@@ -191,88 +254,101 @@ __global__ void __launch_bounds__((Cfg<R, DIM, ORDER, NS, MIX>::NT_GRAD))
       if (en >= E || kn >= NP) {
         atomicOr(a.status, ST_BAD_INDEX);
 #pragma unroll
-        for (int c = 0; c < NU; ++c) up[c] = u_s[(c * EPB + e) * NP + k];
+        for (int c = 0; c < NU; ++c) up[c] = bu[(c * EPB + e) * KU + k];
       } else {
         const int64_t gi = (int64_t)en * NP + kn;
 #pragma unroll
         for (int c = 0; c < NC; ++c) up[c] = a.q[c * EN + gi];
-        up[NC] = MIX ? a.t_op[gi] : node_temperature<R, DIM, NS>(up, (R)0, g);
+        up[NC] = MIX ? a.t_op[gi] : node_temperature<double, DIM, NS>(up, 0.0, g);
       }
     } else {
       const int bf = -(cn + 1);
       const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
       if (kind == BK_PRESCRIBED) {
-        const int64_t bs = (int64_t)a.nbf * NFP;
+        const int64_t bstride = (int64_t)a.nbf * NFP;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) up[c] = a.bext[c * bs + (int64_t)bf * NFP + m];
-        up[NC] = MIX ? a.bext[NC * bs + (int64_t)bf * NFP + m]
-                     : node_temperature<R, DIM, NS>(up, (R)0, g);
-        central = false;   // gradient flux sends the exterior value
+        for (int c = 0; c < NC; ++c) up[c] = a.bext[c * bstride + (int64_t)bf * NFP + m];
+        up[NC] = MIX ? a.bext[NC * bstride + (int64_t)bf * NFP + m]
+                     : node_temperature<double, DIM, NS>(up, 0.0, g);
+        central = false;   // the gradient flux sends the exterior value
       } else {
         if (kind < 0) atomicOr(a.status, ST_BAD_INDEX);
 #pragma unroll
-        for (int c = 0; c < NU; ++c) up[c] = u_s[(c * EPB + e) * NP + k];
+        for (int c = 0; c < NU; ++c) up[c] = bu[(c * EPB + e) * KU + k];
       }
     }
 #pragma unroll
     for (int c = 0; c < NU; ++c) {
-      const R um = u_s[(c * EPB + e) * NP + k];
-      const R ustar = central ? (up[c] + um) / (R)2 : up[c];
-      f_s[(c * EPB + e) * NFN + fm] = fsc * ustar;
+      const double um = bu[(c * EPB + e) * KU + k];
+      const double ustar = central ? (up[c] + um) / 2 : up[c];
+      bs[(c * EPB + e) * KS + f * NFP4 + m] = fsc * ustar;
     }
   }
   __syncthreads();
 
-  // phase 4: one thread per (element, field)
-  for (int p = threadIdx.x; p < EPB * NU; p += blockDim.x) {
-    const int e = p % EPB, c = p / EPB;
-    if (e >= ne) continue;
-    R uk[NP];
-    R sk[NFN];
-#pragma unroll
-    for (int k = 0; k < NP; ++k) uk[k] = u_s[(c * EPB + e) * NP + k];
-#pragma unroll
-    for (int k = 0; k < NFN; ++k) sk[k] = f_s[(c * EPB + e) * NFN + k];
-    R rxe[DIM][DIM], nre[NF][DIM];
+  // phase 4: per 8-column tile, du_r = W_r U and L_f = LIFT_f S on the
+  // float64 tensor cores, then grad_j = sum_f n_fj L_f - sum_r rx_rj du_r
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gq = lane >> 2, tq = lane & 3;
+  for (int nt = warp; nt < NCOL / 8; nt += blockDim.x >> 5) {
+    double du[DIM][MT][2], lf[NF][MT][2];
 #pragma unroll
     for (int r = 0; r < DIM; ++r)
 #pragma unroll
-      for (int j = 0; j < DIM; ++j) rxe[r][j] = rx_s[e * DIM * DIM + r * DIM + j];
+      for (int t = 0; t < MT; ++t) du[r][t][0] = du[r][t][1] = 0.0;
 #pragma unroll
     for (int f = 0; f < NF; ++f)
 #pragma unroll
-      for (int j = 0; j < DIM; ++j) nre[f][j] = nrm_s[(e * NF + f) * DIM + j];
-    R* outp = a.out + ((int64_t)c * DIM) * EN + (int64_t)(e0 + e) * NP;
-    // operands stay in registers; the row index is warp-uniform, so the
-    // reference-matrix entries are broadcast constant loads
-#pragma unroll 1
-    for (int i = 0; i < NP; ++i) {
-      R du[DIM];
+      for (int t = 0; t < MT; ++t) lf[f][t][0] = lf[f][t][1] = 0.0;
+    const double* bcol = bu + (nt * 8 + gq) * KU + tq;
 #pragma unroll
-      for (int r = 0; r < DIM; ++r) {
-        R acc = 0;
+    for (int ks = 0; ks < KU / 4; ++ks) {
+      if (ks * 4 >= NP) break;
+      const double b = bcol[ks * 4];
 #pragma unroll
-        for (int k = 0; k < NP; ++k)
-          acc += RefBank<R>::get(S::OFF_W + (r * NP + i) * NP + k) * uk[k];
-        du[r] = acc;
-      }
-      R lf[NF];
+      for (int r = 0; r < DIM; ++r)
 #pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        R acc = 0;
+        for (int t = 0; t < MT; ++t)
+          dmma884(du[r][t], aw[(r * MP + t * 8 + gq) * KU + ks * 4 + tq], b);
+    }
+    const double* scol = bs + (nt * 8 + gq) * KS + tq;
 #pragma unroll
-        for (int m = 0; m < NFP; ++m)
-          acc += RefBank<R>::get(S::OFF_LIFT + i * NFN + f * NFP + m) * sk[f * NFP + m];
-        lf[f] = acc;
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int ks = 0; ks < NFP4 / 4; ++ks) {
+        const double b = scol[f * NFP4 + ks * 4];
+#pragma unroll
+        for (int t = 0; t < MT; ++t)
+          dmma884(lf[f][t], al[(f * MP + t * 8 + gq) * KL + ks * 4 + tq], b);
       }
 #pragma unroll
-      for (int j = 0; j < DIM; ++j) {
-        R gsum = 0;
+    for (int h = 0; h < 2; ++h) {
+      const int col = nt * 8 + 2 * tq + h;
+      const int c = col / EPB, e = col % EPB;
+      if (c >= NU || e >= ne) continue;
+      double rxe[DIM][DIM], nre[NF][DIM];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) gsum += nre[f][j] * lf[f];
+      for (int r = 0; r < DIM; ++r)
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) gsum -= rxe[r][j] * du[r];
-        outp[(int64_t)j * EN + i] = gsum;
+        for (int j = 0; j < DIM; ++j) rxe[r][j] = rx_s[e * DIM * DIM + r * DIM + j];
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) nre[f][j] = nrm_s[(e * NF + f) * DIM + j];
+      double* outp = a.out + ((int64_t)c * DIM) * EN + (int64_t)(e0 + e) * NP;
+#pragma unroll
+      for (int t = 0; t < MT; ++t) {
+        const int i = t * 8 + gq;
+        if (i >= NP) continue;
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) {
+          double gsum = 0.0;
+#pragma unroll
+          for (int f = 0; f < NF; ++f) gsum += nre[f][j] * lf[f][t][h];
+#pragma unroll
+          for (int r = 0; r < DIM; ++r) gsum -= rxe[r][j] * du[r][t][h];
+          outp[(int64_t)j * EN + i] = gsum;
+        }
       }
     }
   }
@@ -282,22 +358,22 @@ __global__ void __launch_bounds__((Cfg<R, DIM, ORDER, NS, MIX>::NT_GRAD))
 
 // {{{ rhs kernel (Euler when VISC is false)
 
-template <class R, int DIM, int ORDER, int NS, bool MIX, bool VISC>
-__global__ void __launch_bounds__((Cfg<R, DIM, ORDER, NS, MIX>::NT_RHS))
-    k_rhs(DGArgs<R> a, GasParams g) {
-  using C = Cfg<R, DIM, ORDER, NS, MIX>;
+template <int DIM, int ORDER, int NS, bool MIX, bool VISC>
+__global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_rhs(DGArgs<double> a, GasParams g) {
+  using C = Cfg<DIM, ORDER, NS, MIX>;
   using S = Simplex<DIM, ORDER>;
-  constexpr int NP = C::NP, NF = C::NF, NFP = C::NFP, NFN = C::NFN, NC = C::NC, NU = C::NU;
-  constexpr int EPB = C::EPB_RHS;
+  constexpr int NP = C::NP, NF = C::NF, NFP = C::NFP, NFN = C::NFN, NC = C::NC;
+  constexpr int EPB = C::EPB_RHS, MP = C::MP, MT = C::MT, KB = C::KB, KR = C::KR;
+  constexpr int NCOL = C::NCOL_R;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* q_s = reinterpret_cast<R*>(smem_raw);                 // [NC][EPB][NP]
-  R* t_s = q_s + NC * EPB * NP;                            // [2][EPB][NP] (MIX)
-  R* g_s = t_s + (MIX ? 2 * EPB * NP : 0);                 // [DIM][NC][EPB][NP]
-  R* f_s = g_s + DIM * NC * EPB * NP;                      // [NC][EPB][NFN]
-  R* src_s = f_s + NC * EPB * NFN;                         // [NS][EPB][NP]
-  R* rx_s = src_s + NS * EPB * NP;                         // [EPB][DIM][DIM]
-  R* nrm_s = rx_s + EPB * DIM * DIM;
-  R* fs_s = nrm_s + EPB * NF * DIM;
+  double* am = reinterpret_cast<double*>(smem_raw);        // [MP][KB]
+  double* bm = am + MP * KB;                               // [NCOL][KB]
+  double* q_s = bm + NCOL * KB;                            // [NC][EPB][NP]
+  double* t_s = q_s + NC * EPB * NP;                       // [2][EPB][NP] (MIX)
+  double* src_s = t_s + (MIX ? 2 * EPB * NP : 0);          // [NS][EPB][NP] (MIX)
+  double* rx_s = src_s + NS * EPB * NP;                    // [EPB][DIM][DIM]
+  double* nrm_s = rx_s + EPB * DIM * DIM;
+  double* fs_s = nrm_s + EPB * NF * DIM;
   int* fn_s = reinterpret_cast<int*>(fs_s + EPB * NF);
   uint8_t* perm_s = reinterpret_cast<uint8_t*>(fn_s + NFN);
 
@@ -307,6 +383,21 @@ __global__ void __launch_bounds__((Cfg<R, DIM, ORDER, NS, MIX>::NT_RHS))
   const int64_t EN = (int64_t)E * NP;
   const bool sources = MIX && a.add_sources;
 
+  // A = [-W_0 .. -W_{DIM-1} | LIFT], zero padded
+  for (int i = threadIdx.x; i < MP * KB; i += blockDim.x) {
+    const int row = i / KB, k = i % KB;
+    double v = 0.0;
+    if (row < NP && k < KR) {
+      if (k < DIM * NP) {
+        const int r = k / NP, kk = k % NP;
+        v = -c_ref64[S::OFF_W + (r * NP + row) * NP + kk];
+      } else {
+        v = c_ref64[S::OFF_LIFT + row * NFN + (k - DIM * NP)];
+      }
+    }
+    am[i] = v;
+  }
+  for (int i = threadIdx.x; i < NCOL * KB; i += blockDim.x) bm[i] = 0.0;
   for (int i = threadIdx.x; i < NFN; i += blockDim.x) fn_s[i] = c_face_nodes<DIM, ORDER>(i);
   for (int i = threadIdx.x; i < a.nperm * NFP; i += blockDim.x) perm_s[i] = a.perm[i];
   for (int c = 0; c < NC; ++c)
@@ -315,27 +406,27 @@ __global__ void __launch_bounds__((Cfg<R, DIM, ORDER, NS, MIX>::NT_RHS))
   if (MIX)
     for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
       t_s[idx] = a.t_op[(int64_t)e0 * NP + idx];
-      t_s[EPB * NP + idx] = sources ? a.t_src[(int64_t)e0 * NP + idx] : (R)0;
+      t_s[EPB * NP + idx] = sources ? a.t_src[(int64_t)e0 * NP + idx] : 0.0;
     }
-  load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
+  load_geometry<double, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
   __syncthreads();
 
-  // phase 2: volume flux F = F_V - F_I, metric-combined
+  // phase 2: volume flux F = F_V - F_I, metric-combined into B[col][r*NP + k]
   for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
-    const int e = idx / NP;
-    R qq[NC];
+    const int e = idx / NP, k = idx % NP;
+    double qq[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) qq[c] = q_s[(c * EPB) * NP + idx];
-    NodeState<R, DIM, NS> st;
-    make_state<R, DIM, NS>(qq, MIX ? t_s[idx] : (R)0, g, st);
-    R fl[NC][DIM];
-    inviscid_flux<R, DIM, NS>(st, fl);
+    NodeState<double, DIM, NS> st;
+    make_state<double, DIM, NS>(qq, MIX ? t_s[idx] : 0.0, g, st);
+    double fl[NC][DIM];
+    inviscid_flux<double, DIM, NS>(st, fl);
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
       for (int j = 0; j < DIM; ++j) fl[c][j] = -fl[c][j];
     if (VISC) {
-      R gq[NC][DIM], gt[DIM];
+      double gq[NC][DIM], gt[DIM];
       const int64_t gi = (int64_t)e0 * NP + idx;
 #pragma unroll
       for (int c = 0; c < NC; ++c)
@@ -343,69 +434,69 @@ __global__ void __launch_bounds__((Cfg<R, DIM, ORDER, NS, MIX>::NT_RHS))
         for (int j = 0; j < DIM; ++j) gq[c][j] = a.grad[((int64_t)c * DIM + j) * EN + gi];
 #pragma unroll
       for (int j = 0; j < DIM; ++j) gt[j] = a.grad[((int64_t)NC * DIM + j) * EN + gi];
-      R fv[NC][DIM];
-      viscous_flux<R, DIM, NS, MIX>(st, gq, gt, fv);
+      double fv[NC][DIM];
+      viscous_flux<double, DIM, NS, MIX>(st, gq, gt, fv);
 #pragma unroll
       for (int c = 0; c < NC; ++c)
 #pragma unroll
         for (int j = 0; j < DIM; ++j) fl[c][j] = fv[c][j] + fl[c][j];
     }
 #pragma unroll
-    for (int r = 0; r < DIM; ++r)
+    for (int c = 0; c < NC; ++c)
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        R acc = 0;
+      for (int r = 0; r < DIM; ++r) {
+        double acc = 0.0;
 #pragma unroll
         for (int j = 0; j < DIM; ++j) acc += rx_s[e * DIM * DIM + r * DIM + j] * fl[c][j];
-        g_s[((r * NC + c) * EPB) * NP + idx] = acc;
+        bm[(c * EPB + e) * KB + r * NP + k] = acc;
       }
     if constexpr (MIX && NS > 0) {
       if (sources) {
-        R om[NS];
-        const R tsrc = t_s[EPB * NP + idx];
-        production_rates<R, NS>(st.rho, tsrc, st.y, (R)g.zero_level, om);
+        double om[NS];
+        production_rates<double, NS>(st.rho, t_s[EPB * NP + idx], st.y, g.zero_level, om);
 #pragma unroll
-        for (int k = 0; k < NS; ++k) src_s[(k * EPB) * NP + idx] = (R)c_mech.mw[k] * om[k];
+        for (int s = 0; s < NS; ++s) src_s[(s * EPB) * NP + idx] = c_mech.mw[s] * om[s];
       }
     }
   }
   __syncthreads();
 
-  // phase 3: numerical face flux  fscale * (F*_V - F*_I)
+  // phase 3: numerical face flux fscale * (F*_V - F*_I) into B[col][DIM*NP + fm]
   for (int idx = threadIdx.x; idx < ne * NFN; idx += blockDim.x) {
     const int e = idx / NFN, fm = idx % NFN, f = fm / NFP, m = fm % NFP;
     const int k = fn_s[fm];
     const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
-    const R fsc = fs_s[e * NF + f];
-    R n[DIM];
+    const double fsc = fs_s[e * NF + f];
+    double n[DIM];
 #pragma unroll
     for (int j = 0; j < DIM; ++j) n[j] = nrm_s[(e * NF + f) * DIM + j];
-    R qm[NC], qp[NC];
+    double qm[NC], qp[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) qm[c] = q_s[(c * EPB + e) * NP + k];
-    NodeState<R, DIM, NS> sm, sp;
-    make_state<R, DIM, NS>(qm, MIX ? t_s[e * NP + k] : (R)0, g, sm);
-    // own total flux . n from the metric-combined volume flux
-    R nmag2 = 0;
+    NodeState<double, DIM, NS> sm, sp;
+    make_state<double, DIM, NS>(qm, MIX ? t_s[e * NP + k] : 0.0, g, sm);
+    // own total flux . n from the metric-combined volume flux:
+    // F.n = (sum_r N_r G_r) / |rx^T N|
+    double nmag2 = 0.0;
 #pragma unroll
     for (int j = 0; j < DIM; ++j) {
-      R a2 = 0;
+      double a2 = 0.0;
 #pragma unroll
       for (int r = 0; r < DIM; ++r)
-        a2 += rx_s[e * DIM * DIM + r * DIM + j] * RefBank<R>::get(S::OFF_NREF + f * DIM + r);
+        a2 += rx_s[e * DIM * DIM + r * DIM + j] * c_ref64[S::OFF_NREF + f * DIM + r];
       nmag2 += a2 * a2;
     }
-    const R inmag = (R)1 / sqrt(nmag2);
-    R ftm[NC];
+    const double inmag = 1.0 / sqrt(nmag2);
+    double ftm[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      R acc = 0;
+      double acc = 0.0;
 #pragma unroll
       for (int r = 0; r < DIM; ++r)
-        acc += RefBank<R>::get(S::OFF_NREF + f * DIM + r) * g_s[((r * NC + c) * EPB + e) * NP + k];
+        acc += c_ref64[S::OFF_NREF + f * DIM + r] * bm[(c * EPB + e) * KB + r * NP + k];
       ftm[c] = acc * inmag;
     }
-    int mode = 0;   // 0 interior, 1 dummy (copy interior), 2 prescribed
+    int mode = 0;   // 0 interior, 1 dummy (interior only), 2 prescribed exterior
     int64_t gi = 0;
     if (cn >= 0) {
       const int en = cn >> 8, pr = cn & 255;
@@ -417,109 +508,95 @@ __global__ void __launch_bounds__((Cfg<R, DIM, ORDER, NS, MIX>::NT_RHS))
         gi = (int64_t)en * NP + kn;
 #pragma unroll
         for (int c = 0; c < NC; ++c) qp[c] = a.q[c * EN + gi];
-        make_state<R, DIM, NS>(qp, MIX ? a.t_op[gi] : (R)0, g, sp);
+        make_state<double, DIM, NS>(qp, MIX ? a.t_op[gi] : 0.0, g, sp);
       }
     } else {
       const int bf = -(cn + 1);
       const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
       if (kind == BK_PRESCRIBED) {
         mode = 2;
-        const int64_t bs = (int64_t)a.nbf * NFP;
+        const int64_t bstride = (int64_t)a.nbf * NFP;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) qp[c] = a.bext[c * bs + (int64_t)bf * NFP + m];
-        make_state<R, DIM, NS>(qp, MIX ? a.bext[NC * bs + (int64_t)bf * NFP + m] : (R)0, g, sp);
+        for (int c = 0; c < NC; ++c) qp[c] = a.bext[c * bstride + (int64_t)bf * NFP + m];
+        make_state<double, DIM, NS>(qp, MIX ? a.bext[NC * bstride + (int64_t)bf * NFP + m] : 0.0,
+                                    g, sp);
       } else {
         if (kind < 0) atomicOr(a.status, ST_BAD_INDEX);
         mode = 1;
       }
     }
-    R out[NC];
+    double out[NC];
     if (mode == 1) {
       // DummyBoundary: F_V(q-).n - F_I(q-).n  (boundary.py:1027-1049)
 #pragma unroll
       for (int c = 0; c < NC; ++c) out[c] = ftm[c];
     } else {
-      R fi[NC];
-      inviscid_num_flux<R, DIM, NS>(sm, sp, qm, qp, n, a.flux_kind, fi);
+      double fi[NC];
+      inviscid_num_flux<double, DIM, NS>(sm, sp, qm, qp, n, a.flux_kind, fi);
 #pragma unroll
       for (int c = 0; c < NC; ++c) out[c] = -fi[c];
       if (VISC) {
         // own viscous part: F_V- . n = (F_V - F_I)- . n + F_I- . n
-        R fim[NC];
-        inviscid_flux_n<R, DIM, NS>(sm, n, fim);
-        R gq[NC][DIM], gt[DIM];
+        double fim[NC];
+        inviscid_flux_n<double, DIM, NS>(sm, n, fim);
+        double gqp[NC][DIM], gtp[DIM];
         const int64_t gsrc = (mode == 0) ? gi : (int64_t)(e0 + e) * NP + k;
 #pragma unroll
         for (int c = 0; c < NC; ++c)
 #pragma unroll
-          for (int j = 0; j < DIM; ++j) gq[c][j] = a.grad[((int64_t)c * DIM + j) * EN + gsrc];
+          for (int j = 0; j < DIM; ++j) gqp[c][j] = a.grad[((int64_t)c * DIM + j) * EN + gsrc];
 #pragma unroll
-        for (int j = 0; j < DIM; ++j) gt[j] = a.grad[((int64_t)NC * DIM + j) * EN + gsrc];
-        R fvp[NC][DIM];
-        viscous_flux<R, DIM, NS, MIX>(sp, gq, gt, fvp);
+        for (int j = 0; j < DIM; ++j) gtp[j] = a.grad[((int64_t)NC * DIM + j) * EN + gsrc];
+        double fvp[NC][DIM];
+        viscous_flux<double, DIM, NS, MIX>(sp, gqp, gtp, fvp);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          R fvpn = 0;
+          double fvpn = 0.0;
 #pragma unroll
           for (int j = 0; j < DIM; ++j) fvpn += fvp[c][j] * n[j];
-          const R fvmn = ftm[c] + fim[c];
-          out[c] += (fvmn + fvpn) / (R)2;
+          const double fvmn = ftm[c] + fim[c];
+          out[c] += (fvmn + fvpn) / 2;
         }
       }
     }
 #pragma unroll
-    for (int c = 0; c < NC; ++c) f_s[(c * EPB + e) * NFN + fm] = fsc * out[c];
+    for (int c = 0; c < NC; ++c) bm[(c * EPB + e) * KB + DIM * NP + fm] = fsc * out[c];
   }
   __syncthreads();
 
-  // phase 4: rhs = LIFT * S - sum_r W_r G_r  (+ sources)
-  for (int p = threadIdx.x; p < EPB * NC; p += blockDim.x) {
-    const int e = p % EPB, c = p / EPB;
-    if (e >= ne) continue;
-    R acc[NP];
+  // phase 4: rhs = [-W | LIFT] [G ; S] on the float64 tensor cores (+ sources)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gq = lane >> 2, tq = lane & 3;
+  bool bad = false;
+  for (int nt = warp; nt < NCOL / 8; nt += blockDim.x >> 5) {
+    double d[MT][2];
 #pragma unroll
-    for (int i = 0; i < NP; ++i) acc[i] = 0;
+    for (int t = 0; t < MT; ++t) d[t][0] = d[t][1] = 0.0;
+    const double* bcol = bm + (nt * 8 + gq) * KB + tq;
+#pragma unroll 5
+    for (int ks = 0; ks < (KR + 3) / 4; ++ks) {
+      const double b = bcol[ks * 4];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) {
-      R sk[NFP];
+      for (int t = 0; t < MT; ++t) dmma884(d[t], am[(t * 8 + gq) * KB + ks * 4 + tq], b);
+    }
 #pragma unroll
-      for (int m = 0; m < NFP; ++m) sk[m] = f_s[(c * EPB + e) * NFN + f * NFP + m];
+    for (int h = 0; h < 2; ++h) {
+      const int col = nt * 8 + 2 * tq + h;
+      const int c = col / EPB, e = col % EPB;
+      if (c >= NC || e >= ne) continue;
+      double* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
 #pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        R s = 0;
-#pragma unroll
-        for (int m = 0; m < NFP; ++m)
-          s += RefBank<R>::get(S::OFF_LIFT + i * NFN + f * NFP + m) * sk[m];
-        acc[i] += s;
+      for (int t = 0; t < MT; ++t) {
+        const int i = t * 8 + gq;
+        if (i >= NP) continue;
+        double v = d[t][h];
+        if (sources && c >= 2 + DIM) v += src_s[((c - 2 - DIM) * EPB + e) * NP + i];
+        outp[i] = v;
+        bad |= !(v == v);
       }
     }
-#pragma unroll
-    for (int r = 0; r < DIM; ++r) {
-      R gk[NP];
-#pragma unroll
-      for (int k = 0; k < NP; ++k) gk[k] = g_s[((r * NC + c) * EPB + e) * NP + k];
-#pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        R s = 0;
-#pragma unroll
-        for (int k = 0; k < NP; ++k) s += RefBank<R>::get(S::OFF_W + (r * NP + i) * NP + k) * gk[k];
-        acc[i] -= s;
-      }
-    }
-    if (sources && c >= 2 + DIM) {
-      const int sidx = c - 2 - DIM;
-#pragma unroll
-      for (int i = 0; i < NP; ++i) acc[i] += src_s[(sidx * EPB + e) * NP + i];
-    }
-    R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
-    bool bad = false;
-#pragma unroll
-    for (int i = 0; i < NP; ++i) {
-      outp[i] = acc[i];
-      bad |= !(acc[i] == acc[i]);
-    }
-    if (bad) atomicOr(a.status, ST_NAN);
   }
+  if (bad) atomicOr(a.status, ST_NAN);
 }
 
 // }}}

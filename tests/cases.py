@@ -19,14 +19,20 @@ def rel_l2(a, b):
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
 
 
-def field_rel_l2(a, b):
-    """Largest per-field relative L2 error (fields along axis 0)."""
+def field_rel_l2(a, b, floor=None):
+    """Largest per-field relative L2 error (fields along axis 0).
+
+    A field whose reference is zero up to roundoff (e.g. grad(rho) for a
+    uniform density) is measured against ``floor[c]`` (its natural scale)
+    or, by default, 1e-3 of the largest field norm, instead of its own
+    norm."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
-    tot = np.linalg.norm(b.ravel())
+    big = max(np.linalg.norm(b[c].ravel()) for c in range(b.shape[0]))
     errs = []
     for c in range(b.shape[0]):
-        den = max(np.linalg.norm(b[c].ravel()), 1e-6 * tot, 1e-300)
+        fl = 1e-3 * big if floor is None else floor[c]
+        den = max(np.linalg.norm(b[c].ravel()), fl, 1e-300)
         errs.append(np.linalg.norm((a[c] - b[c]).ravel()) / den)
     return float(max(errs))
 
