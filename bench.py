@@ -45,49 +45,82 @@ def _peaks():
 # {{{ workloads
 
 WORKLOADS = {
+    "reacting_p3_tet80": dict(
+        desc="3-D reacting Navier-Stokes, uiuc_7sp ethylene/air (7 species, 3 Arrhenius "
+             "reactions, NASA-7), periodic [0,2pi]^3 m box, 80^3 hexes x 6 tets "
+             "(3,072,000 tets), order 3 (20 nodes/tet), 61.4M nodes x 12 fields; seeded "
+             "smooth random T in [300,2500] K, p = 101325 +-5%, Dirichlet(2) mass "
+             "fractions, |v| <= 10 m/s; SimpleTransport mu = kappa = D = 1e-5; Newton "
+             "seeded with the step-start temperature; reactions on",
+        n=80, order=3, kind="reacting"),
+    "reacting_p2_tet40": dict(
+        desc="3-D reacting Navier-Stokes, uiuc_7sp, 40^3 hexes x 6 tets (384,000 tets), "
+             "order 2 (10 nodes/tet), same fields and models as reacting_p3_tet80",
+        n=40, order=2, kind="reacting"),
     "tgv_p3_tet24": dict(
         desc="3-D viscous Taylor-Green vortex, periodic [-pi,pi]^3, 24^3 hexes x 6 tets "
              "(82,944 tets), order 3 (20 nodes/tet), ideal gas gamma=1.4, Mach 0.1, "
-             "Re 1600, Pr 0.71, Rusanov + BR1, plain FP64",
+             "Re 1600, Pr 0.71, Rusanov + BR1",
         n=24, order=3, kind="tgv"),
 }
+DEFAULT_WORKLOAD = "reacting_p3_tet80"
 
 
 def build_workload(name, device):
     import torch
 
     from mirgecom_b200.discretization import Discretization
-    from mirgecom_b200.eos import IdealSingleGas
+    from mirgecom_b200.eos import IdealSingleGas, PyrometheusMixture
     from mirgecom_b200.gas_model import GasModel
-    from mirgecom_b200.initializers import (taylor_green_state,
+    from mirgecom_b200.initializers import (reacting_mixture_state, taylor_green_state,
                                             taylor_green_transport_params)
     from mirgecom_b200.mesh import generate_box_mesh
+    from mirgecom_b200.thermochemistry import UIUC_7SP
     from mirgecom_b200.transport import SimpleTransport
     w = WORKLOADS[name]
-    mesh = generate_box_mesh((-np.pi,) * 3, (np.pi,) * 3, (w["n"],) * 3,
-                             periodic=(True,) * 3)
+    if w["kind"] == "tgv":
+        mesh = generate_box_mesh((-np.pi,) * 3, (np.pi,) * 3, (w["n"],) * 3,
+                                 periodic=(True,) * 3)
+    else:
+        mesh = generate_box_mesh((0.0,) * 3, (2 * np.pi,) * 3, (w["n"],) * 3,
+                                 periodic=(True,) * 3)
     dcoll = Discretization(mesh, w["order"], device=device)
     x = [t for t in dcoll.nodes(device)]
-    cv = taylor_green_state(x)
-    gas = GasModel(eos=IdealSingleGas(), transport=SimpleTransport(
-        **taylor_green_transport_params()))
+    if w["kind"] == "tgv":
+        cv = taylor_green_state(x)
+        gas = GasModel(eos=IdealSingleGas(), transport=SimpleTransport(
+            **taylor_green_transport_params()))
+        tseed = None
+    else:
+        cv, tseed = reacting_mixture_state(x, UIUC_7SP, seed=0)
+        gas = GasModel(eos=PyrometheusMixture(UIUC_7SP, temperature_niter=5),
+                       transport=SimpleTransport(viscosity=1e-5, thermal_conductivity=1e-5,
+                                                 species_diffusivity=[1e-5] * 7))
+        # the step-start temperature: the exact temperature of a nearby state
+        tseed = tseed + 2.0
+    del x
     torch.cuda.synchronize()
-    return dcoll, cv, gas
+    return dcoll, cv, gas, tseed
 
 
-def algorithmic_bytes(dcoll, nc, s=8):
+def algorithmic_bytes(dcoll, nc, s=8, mixture=False):
     """Compulsory HBM bytes per launch of each kernel of one NS RHS.
 
-    grad: read q (Nc) + write grad ((Nc+1) d) per node, + rx and face
-    pairing per element.  rhs: read q (Nc) + grad ((Nc+1) d), write rhs
-    (Nc) per node, + rx and face pairing per element.
+    state (mixture): read q (Nc) and the seed, write T (1, plus the operator
+    temperature on the float64 path).  grad: read q (Nc) [+ T], write grad
+    ((Nc+1) d) per node.  rhs: read q (Nc) + grad ((Nc+1) d) [+ T, T_src],
+    write rhs (Nc) per node.  Plus rx and the face pairing per element.
     """
     d = dcoll.dim
     nn = dcoll.nelements * dcoll.refel.nnodes
     geo = dcoll.nelements * (d * d * s + dcoll.nfaces * 4)
-    grad = nn * (nc + (nc + 1) * d) * s + geo
-    rhs = nn * (nc + (nc + 1) * d + nc) * s + geo
-    return {"grad": grad, "rhs": rhs}
+    t_in = 1 if mixture else 0
+    grad = nn * (nc + t_in + (nc + 1) * d) * s + geo
+    rhs = nn * (nc + (nc + 1) * d + nc + 2 * t_in) * s + geo
+    out = {"grad": grad, "rhs": rhs}
+    if mixture:
+        out["state"] = nn * (nc + 1 + (2 if s == 8 else 1)) * s
+    return out
 
 # }}}
 
@@ -150,37 +183,73 @@ def _dist_env():
     return rank, world, local
 
 
-def cpu_baseline(name, seconds=10.0):
-    """The float64 oracle (numpy) on a bounded sample of the same physics."""
+def _oracle_sample(name):
+    """Oracle discretization and state on a bounded sample of the workload."""
+    import torch
+
     from mirgecom_b200.discretization import Discretization
+    from mirgecom_b200.initializers import reacting_mixture_state
     from mirgecom_b200.mesh import generate_box_mesh
+    from mirgecom_b200.thermochemistry import UIUC_7SP
     from oracle import dg as odg
     from oracle import physics as oph
     w = WORKLOADS[name]
-    n_sample = 6
-    mesh = generate_box_mesh((-np.pi,) * 3, (np.pi,) * 3, (n_sample,) * 3,
-                             periodic=(True,) * 3)
+    if w["kind"] == "tgv":
+        n_sample = 6
+        mesh = generate_box_mesh((-np.pi,) * 3, (np.pi,) * 3, (n_sample,) * 3,
+                                 periodic=(True,) * 3)
+    else:
+        n_sample = 3
+        mesh = generate_box_mesh((0.0,) * 3, (2 * np.pi,) * 3, (n_sample,) * 3,
+                                 periodic=(True,) * 3)
     d = Discretization(mesh, w["order"])
     od = odg.OracleDisc(mesh, d.refel)
     x = od.nodes
-    u = np.sin(x[0]) * np.cos(x[1]) * np.cos(x[2])
-    v = -np.cos(x[0]) * np.sin(x[1]) * np.cos(x[2])
-    p = 1 / (1.4 * 0.01) + (np.cos(2 * x[0]) + np.cos(2 * x[1])) * (np.cos(2 * x[2]) + 2) / 16
-    q = np.array([np.ones_like(u), p / 0.4 + 0.5 * (u * u + v * v), u, v, 0 * u])
-    mu = 1 / 1600
-    otr = oph.SimpleTransportParams(viscosity=mu, thermal_conductivity=mu * 1004.85 / 0.71)
-    gas = oph.IdealGas()
-    odg.ns_operator(od, oph.make_fluid_state(q, gas, otr, 3), gas, otr, {})
+    if w["kind"] == "tgv":
+        u = np.sin(x[0]) * np.cos(x[1]) * np.cos(x[2])
+        v = -np.cos(x[0]) * np.sin(x[1]) * np.cos(x[2])
+        p = 1 / (1.4 * 0.01) + (np.cos(2 * x[0]) + np.cos(2 * x[1])) * (np.cos(2 * x[2]) + 2) / 16
+        q = np.array([np.ones_like(u), p / 0.4 + 0.5 * (u * u + v * v), u, v, 0 * u])
+        mu = 1 / 1600
+        otr = oph.SimpleTransportParams(viscosity=mu, thermal_conductivity=mu * 1004.85 / 0.71)
+        gas = oph.IdealGas()
+        tseed = None
+    else:
+        cv, t = reacting_mixture_state([torch.from_numpy(x[i]) for i in range(3)],
+                                       UIUC_7SP, seed=0)
+        q = cv.q.numpy()
+        tseed = t.numpy() + 2.0
+        otr = oph.SimpleTransportParams(viscosity=1e-5, thermal_conductivity=1e-5,
+                                        species_diffusivity=(1e-5,) * 7)
+        gas = oph.MixtureGas(UIUC_7SP, temperature_niter=5)
+    return od, q, tseed, gas, otr, mesh.nelements, n_sample
+
+
+def _oracle_rhs(od, q, tseed, gas, otr):
+    from oracle import dg as odg
+    from oracle import physics as oph
+    st = oph.make_fluid_state(q, gas, otr, 3, temperature_seed=tseed)
+    rhs = odg.ns_operator(od, st, gas, otr, {})
+    if isinstance(gas, oph.MixtureGas):
+        rhs = rhs + oph.species_source_terms(gas, q, st["temperature"], 3)
+    return rhs
+
+
+def cpu_baseline(name, seconds=10.0):
+    """The float64 oracle (numpy, one host thread) on a bounded sample of the
+    same physics and order; the sample is stated in the result."""
+    od, q, tseed, gas, otr, nel, n_sample = _oracle_sample(name)
+    _oracle_rhs(od, q, tseed, gas, otr)
     t0 = time.perf_counter()
     reps = 0
     while time.perf_counter() - t0 < seconds or reps < 2:
-        odg.ns_operator(od, oph.make_fluid_state(q, gas, otr, 3), gas, otr, {})
+        _oracle_rhs(od, q, tseed, gas, otr)
         reps += 1
     dt = (time.perf_counter() - t0) / reps
     dof = q.size
     return {"value": dof / dt, "unit": "DOF-RHS/s", "cores": 1, "kind": "port",
-            "sample": f"{n_sample}^3 x 6 tets ({mesh.nelements} tets, {dof} DOF), same "
-                      f"physics and order, {reps} RHS evaluations, numpy float64 oracle"}
+            "sample": f"{n_sample}^3 x 6 tets ({nel} tets, {dof} DOF), same physics and "
+                      f"order as {name}, {reps} RHS evaluations, numpy float64 oracle"}
 
 
 def run_reference(args):
@@ -203,14 +272,44 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _rhs_call(dcoll, gas, q, tseed, events=None):
+    """One RHS evaluation of the workload through the public API."""
+    from mirgecom_b200 import runtime
+    from mirgecom_b200.fluid import ConservedVars
+    from mirgecom_b200.gas_model import make_fluid_state
+    if events:
+        events[0].record()
+    st = make_fluid_state(ConservedVars(q, 3), gas, temperature_seed=tseed)
+    src = st.temperature if st.is_mixture else None
+    rhs, _ = runtime.ns_rhs(dcoll, st, gas, {}, 0.0, 0, source_temperature=src,
+                            events=events[1:] if events else None)
+    return rhs
+
+
+def _time_form(dcoll, gas, q, tseed, steps, warmup, flush, stream):
+    import torch
+    for _ in range(warmup):
+        _rhs_call(dcoll, gas, q, tseed)
+    torch.cuda.synchronize()
+    evs = []
+    for i in range(steps):
+        flush.fill_(float(i))
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        _rhs_call(dcoll, gas, q, tseed, events=ev)
+        evs.append(ev)
+    torch.cuda.synchronize()
+    step_ms = [e[0].elapsed_time(e[3]) for e in evs]
+    kern = {"state": float(np.mean([e[0].elapsed_time(e[1]) for e in evs])),
+            "grad": float(np.mean([e[1].elapsed_time(e[2]) for e in evs])),
+            "rhs": float(np.mean([e[2].elapsed_time(e[3]) for e in evs]))}
+    return float(np.sum(step_ms)), kern
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
 
     from mirgecom_b200 import runtime
-    from mirgecom_b200.fluid import ConservedVars
-    from mirgecom_b200.gas_model import make_fluid_state
-    from mirgecom_b200.navierstokes import ns_operator
 
     rank, world, local = _dist_env()
     if world > 1:
@@ -218,104 +317,97 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    dcoll, cv, gas = build_workload(args.workload, dev)
-    q = cv.q.contiguous()
-    nc = q.shape[0]
-    dof = q.numel()
+    w = WORKLOADS[args.workload]
+    mixture = w["kind"] == "reacting"
+    dcoll, cv, gas, tseed = build_workload(args.workload, dev)
+    q64 = cv.q.contiguous()
+    q32 = q64.to(torch.float32)
+    t64 = tseed.contiguous() if mixture else None
+    t32 = tseed.to(torch.float32) if mixture else None
+    nc = q64.shape[0]
+    dof = q64.numel()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    def step(qq):
-        st = make_fluid_state(ConservedVars(qq, 3), gas)
-        return ns_operator(dcoll, gas, st, {})
-
-    for _ in range(args.warmup):
-        step(q)
-    torch.cuda.synchronize()
-    if runtime.read_status(dcoll, dev) != 0:
-        raise RuntimeError("device status error during warm-up")
-
-    # timed region: K steps, per-step events, L2 flush between steps
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    kev = []
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        for i in range(args.steps):
-            flush.fill_(float(i))
-            kern = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-            ev[i][0].record(stream)
-            runtime.ns_rhs(dcoll, make_fluid_state(ConservedVars(q, 3), gas), gas, {}, 0.0,
-                           0, events=kern)
-            ev[i][1].record(stream)
-            kev.append(kern)
-        torch.cuda.synchronize()
+        ms64, k64 = _time_form(dcoll, gas, q64, t64, args.steps, args.warmup, flush, stream)
+        ms32, k32 = _time_form(dcoll, gas, q32, t32, args.steps, args.warmup, flush, stream)
     if world > 1:
         dist.barrier()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    grad_ms = [k[0].elapsed_time(k[1]) for k in kev]
-    rhs_ms = [k[1].elapsed_time(k[2]) for k in kev]
-    total_ms = float(np.sum(step_ms))
+    status = runtime.read_status(dcoll, dev)
     if world > 1:
-        t = torch.tensor([total_ms], device=dev)
+        t = torch.tensor([ms64, ms32], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
-    value = world * dof * args.steps / (total_ms / 1e3)
+        ms64, ms32 = [float(v) for v in t.tolist()]
+    value64 = world * dof * args.steps / (ms64 / 1e3)
+    value32 = world * dof * args.steps / (ms32 / 1e3)
 
-    # end to end through the public API with host buffers
-    q_host = q.cpu().pin_memory()
+    # end to end through the public API with host buffers (mixed form: the
+    # float32 state goes in, the float32 right-hand side comes out)
+    q_host = q32.cpu().pin_memory()
     out_host = torch.empty_like(q_host).pin_memory()
-    qd = torch.empty_like(q)
-    e2e_ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    qd = torch.empty_like(q32)
     for _ in range(2):
         qd.copy_(q_host, non_blocking=True)
-        out_host.copy_(step(qd).q, non_blocking=True)
+        out_host.copy_(_rhs_call(dcoll, gas, qd, t32), non_blocking=True)
     torch.cuda.synchronize()
     e2e_ms = 0.0
+    ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
     for i in range(args.steps):
         flush.fill_(float(i))
-        e2e_ev[0].record(stream)
+        ev[0].record(stream)
         qd.copy_(q_host, non_blocking=True)
-        out_host.copy_(step(qd).q, non_blocking=True)
-        e2e_ev[1].record(stream)
+        out_host.copy_(_rhs_call(dcoll, gas, qd, t32), non_blocking=True)
+        ev[1].record(stream)
         torch.cuda.synchronize()
-        e2e_ms += e2e_ev[0].elapsed_time(e2e_ev[1])
+        e2e_ms += ev[0].elapsed_time(ev[1])
     e2e_value = world * dof * args.steps / (e2e_ms / 1e3)
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel of the headline (mixed) form
     hbm, peak_kind = _peaks()
-    ab = algorithmic_bytes(dcoll, nc)
-    kt = {"grad": float(np.mean(grad_ms)), "rhs": float(np.mean(rhs_ms))}
+    ab = algorithmic_bytes(dcoll, nc, s=4, mixture=mixture)
+    kt = {k: v for k, v in k32.items() if k in ab}
     top = max(kt, key=kt.get)
     achieved = ab[top] / (kt[top] / 1e3) / 1e9
+    ab64 = algorithmic_bytes(dcoll, nc, s=8, mixture=mixture)
+    kt64 = {k: v for k, v in k64.items() if k in ab64}
+    top64 = max(kt64, key=kt64.get)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(args.workload, {}).get(top)
+            traffic = json.load(f).get(args.workload, {}).get("mixed_" + top)
 
     if rank != 0:
         return
     cpu = cpu_baseline(args.workload) if world == 1 and not args.no_cpu else None
+    launches_per_step = 3 if mixture else 2
     line = {
-        "metric": "DOF-RHS evals/s", "value": value, "unit": "DOF-RHS/s",
+        "metric": "DOF-RHS evals/s", "value": value32, "unit": "DOF-RHS/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"],
+        "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+tf32x3 (f64 Newton residual, f64 sources)",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "desc": w["desc"],
                    "elements": dcoll.nelements, "dof": dof,
+                   "form": "mixed precision, plain-guess Newton",
                    "l2": "flushed between timed steps (512 MiB write, untimed)",
                    "parallelism": f"replicas x{world}"},
+        "plain_fp64": {"value": value64, "ms_per_step": ms64 / args.steps, "kernels_ms": k64,
+                       "roofline_frac": ab64[top64] / (kt64[top64] / 1e3) / 1e9 / hbm,
+                       "dominant_kernel": top64},
+        "mixed_over_fp64": value32 / value64,
+        "kernels_ms": k32,
         "e2e": {"value": e2e_value, "unit": "DOF-RHS/s",
-                "h2d_bytes_per_step": q.numel() * 8, "d2h_bytes_per_step": q.numel() * 8},
-        "gpu_launches": 2 * args.steps,
-        "kernels_ms": kt,
+                "h2d_bytes_per_step": q32.numel() * 4, "d2h_bytes_per_step": q32.numel() * 4},
+        "gpu_launches": 2 * launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                      "algorithmic_bytes": ab[top], "traffic": traffic},
+        "device_status": status,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
@@ -327,10 +419,10 @@ def run_ours(args):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tgv_p3_tet24", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args(argv)
     if args.impl == "reference":

@@ -99,6 +99,7 @@ typedef struct {
   const int32_t* conn;
   const uint8_t* perm;
   const int8_t* bkind;
+  const float* rx32;        /* float32 copy of rx, for the *_f32 entry points */
 } mgc_mesh_t;
 
 /* Library version and the list of supported (dim, order) pairs. */
@@ -153,6 +154,41 @@ int mgc_ns_rhs(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
 int mgc_rk4_stage(int64_t n, const double* q0, const double* k, double* sum,
                   double* q_out, float* q_out_lo, int stage, double dt,
                   void* stream);
+
+/* ---- mixed-precision form (float32 storage and pointwise math, tf32 x3
+ * tensor-core contractions with float32 accumulation).  Same semantics and
+ * layouts as the float64 entry points above, with float arrays; the
+ * operator temperature t_op is the single temperature of the state. ---- */
+
+int mgc_euler_rhs_f32(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
+                      const float* t_op, const float* bext, int flux_kind, float* rhs,
+                      int32_t* status, void* stream);
+
+int mgc_ns_grad_f32(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
+                    const float* t_op, const float* bext, float* grad, int32_t* status,
+                    void* stream);
+
+int mgc_ns_rhs_f32(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
+                   const float* t_op, const float* t_src, const float* grad,
+                   const float* bext, int flux_kind, int add_sources, float* rhs,
+                   int32_t* status, void* stream);
+
+/* Mixture temperature, mixed form: float32 Newton with an adaptive stop,
+ * started from t_guess (the learned guess; NULL to start from t_seed), a
+ * float64 residual check |e - e(T)| / (c_v T) <= rtol, and the plain guess
+ * t_seed as fallback when the check fails.  iters (nullable) receives the
+ * iteration count per node (+1000 when the fallback ran); nodes failing
+ * both set MGC_ST_NEWTON_MISS. */
+int mgc_mixture_temperature_f32(int dim, const mgc_gas_t* gas, int64_t nnodes,
+                                const float* q, const float* t_seed, const float* t_guess,
+                                float* t_out, int32_t* iters, int maxit, float rtol,
+                                int32_t* status, void* stream);
+
+/* rk4 stage with a float32 right-hand side k: the state and the stage sum
+ * stay float64, q_out_lo receives the float32 copy of q_out. */
+int mgc_rk4_stage_mixed(int64_t n, const double* q0, const float* k, double* sum,
+                        double* q_out, float* q_out_lo, int stage, double dt,
+                        void* stream);
 
 #ifdef __cplusplus
 }

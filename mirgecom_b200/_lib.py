@@ -62,7 +62,7 @@ class MeshStruct(C.Structure):
         ("dim", C.c_int32), ("order", C.c_int32), ("nelem", C.c_int32),
         ("nbf", C.c_int32), ("nperm", C.c_int32), ("pad_", C.c_int32),
         ("rx", C.c_void_p), ("conn", C.c_void_p), ("perm", C.c_void_p),
-        ("bkind", C.c_void_p),
+        ("bkind", C.c_void_p), ("rx32", C.c_void_p),
     ]
 
 
@@ -78,6 +78,12 @@ _SIGNATURES = {
     "mgc_ns_grad": ([_P, _P, _P, _P, _P, _P, _P, _P], C.c_int),
     "mgc_ns_rhs": ([_P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P], C.c_int),
     "mgc_rk4_stage": ([C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_double, _P], C.c_int),
+    "mgc_euler_rhs_f32": ([_P, _P, _P, _P, _P, C.c_int, _P, _P, _P], C.c_int),
+    "mgc_ns_grad_f32": ([_P, _P, _P, _P, _P, _P, _P, _P], C.c_int),
+    "mgc_ns_rhs_f32": ([_P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P], C.c_int),
+    "mgc_mixture_temperature_f32": (
+        [C.c_int, _P, C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_float, _P, _P], C.c_int),
+    "mgc_rk4_stage_mixed": ([C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_double, _P], C.c_int),
 }
 
 _lib = None

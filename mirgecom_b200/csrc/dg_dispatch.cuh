@@ -42,12 +42,12 @@ inline int prepare_kernel(Kern kern, size_t smem) {
   return MGC_OK;
 }
 
-template <int DIM, int ORDER, int NS, bool MIX>
+template <class R, int DIM, int ORDER, int NS, bool MIX>
 struct Launch {
-  using C = Cfg<DIM, ORDER, NS, MIX>;
-  static int grad(const DGArgs<double>& a, const GasParams& g, cudaStream_t s) {
+  using C = Cfg<R, DIM, ORDER, NS, MIX>;
+  static int grad(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
     const size_t smem = C::smem_grad(a.nperm);
-    auto kern = k_grad<DIM, ORDER, NS, MIX>;
+    auto kern = k_grad<R, DIM, ORDER, NS, MIX>;
     int rc = prepare_kernel(kern, smem);
     if (rc) return rc;
     const int nblk = (a.nelem + C::EPB_GRAD - 1) / C::EPB_GRAD;
@@ -55,9 +55,9 @@ struct Launch {
     return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
   }
   template <bool VISC>
-  static int rhs(const DGArgs<double>& a, const GasParams& g, cudaStream_t s) {
+  static int rhs(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
     const size_t smem = C::smem_rhs(a.nperm);
-    auto kern = k_rhs<DIM, ORDER, NS, MIX, VISC>;
+    auto kern = k_rhs<R, DIM, ORDER, NS, MIX, VISC>;
     int rc = prepare_kernel(kern, smem);
     if (rc) return rc;
     const int nblk = (a.nelem + C::EPB_RHS - 1) / C::EPB_RHS;
@@ -72,21 +72,45 @@ inline int dispatch_order(int op, int ns, bool mix, const DGArgs<R>& a, const Ga
                           cudaStream_t s) {
 #define MGC_CASE(NSV, MIXV)                                              \
   if (ns == NSV && mix == MIXV) {                                        \
-    using L = Launch<DIM, ORDER, NSV, MIXV>;                             \
+    using L = Launch<R, DIM, ORDER, NSV, MIXV>;                          \
     if (op == 0) return L::grad(a, g, s);                                \
     if (op == 1) return L::template rhs<false>(a, g, s);                 \
     return L::template rhs<true>(a, g, s);                               \
   }
-  MGC_CASE(0, false)
-  MGC_CASE(2, false)
-  MGC_CASE(7, false)
-  MGC_CASE(7, true)
+  if constexpr (sizeof(R) == 8) {
+    MGC_CASE(0, false)
+    MGC_CASE(2, false)
+    MGC_CASE(7, false)
+    MGC_CASE(7, true)
+  } else {
+    MGC_CASE(0, false)
+    MGC_CASE(7, true)
+  }
 #undef MGC_CASE
   return MGC_E_UNSUPPORTED;
 }
 
 inline bool supported_species(int ns, bool mix) {
   return (ns == 0 && !mix) || (ns == 2 && !mix) || (ns == 7);
+}
+
+inline bool supported_species_f32(int ns, bool mix) {
+  return (ns == 0 && !mix) || (ns == 7 && mix);
+}
+
+template <int DIM>
+inline int mixture_state_mixed_dim(int ns, int64_t nnodes, const float* q, const float* tseed,
+                                   const float* tguess, float* tout, int32_t* iters, int maxit,
+                                   float rtol, int32_t* status, const GasParams& g,
+                                   cudaStream_t s) {
+  if (ns != 7) return MGC_E_UNSUPPORTED;
+  const int nt = 256;
+  int64_t nb = (nnodes + nt - 1) / nt;
+  if (nb > 148 * 16) nb = 148 * 16;
+  if (nb < 1) nb = 1;
+  k_mixture_state_mixed<DIM, 7><<<(unsigned)nb, nt, 0, s>>>(nnodes, q, tseed, tguess, tout, iters,
+                                                           maxit, rtol, status, g);
+  return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
 }
 
 template <class R, int DIM>

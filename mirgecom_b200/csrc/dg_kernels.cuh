@@ -56,62 +56,84 @@ struct DGArgs {
 
 enum BoundaryKind { BK_DUMMY = 0, BK_PRESCRIBED = 1 };
 
+
 __host__ __device__ constexpr int imin(int a, int b) { return a < b ? a : b; }
 __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
-// Padded row stride (in doubles) of a shared-memory operand matrix read as
-// m8n8k4 f64 MMA fragments: rows hold K entries (rounded to the k-step 4),
-// and stride = 4 (mod 16) keeps each half-warp's 16 loads on distinct banks.
-__host__ __device__ constexpr int mma_stride(int k) {
-  return round_up(k, 4) + ((4 - round_up(k, 4) % 16) + 16) % 16;
-}
+// Tensor-core tiling per arithmetic type.
+//   double: mma.m8n8k4.f64        -- m-tile 8,  k-step 4, 8-byte banks;
+//   float : mma.m16n8k8.tf32 x 3  -- m-tile 16, k-step 8, 4-byte banks.
+// A row stride of MODK (mod 2*KSTEP... see mma_stride) keeps every fragment
+// load of a warp (8 rows x 4 consecutive k) on distinct shared-memory banks.
+template <class R> struct Tile;
+template <> struct Tile<double> {
+  static constexpr int MROW = 8, KSTEP = 4;
+  // stride = 4 (mod 8) doubles: rows g=0..3 of a half-warp hit 4 disjoint bank quads
+  static constexpr __host__ __device__ int stride(int k) {
+    return round_up(k, 4) % 8 == 4 ? round_up(k, 4) : round_up(k, 4) + 4;
+  }
+};
+template <> struct Tile<float> {
+  static constexpr int MROW = 16, KSTEP = 8;
+  // stride = 4 (mod 8) floats: rows g=0..7 x 4 consecutive k cover 32 banks
+  static constexpr __host__ __device__ int stride(int k) {
+    return round_up(k, 8) + 4;
+  }
+};
 
-template <int DIM, int ORDER, int NS, bool MIX>
+template <class R, int DIM, int ORDER, int NS, bool MIX>
 struct Cfg {
   using S = Simplex<DIM, ORDER>;
+  using T = Tile<R>;
+  static constexpr int RB = (int)sizeof(R);
+  static constexpr bool TF32 = sizeof(R) == 4;
   static constexpr int NP = S::NP, NF = S::NF, NFP = S::NFP;
   static constexpr int NFN = NF * NFP;
   static constexpr int NC = DIM + 2 + NS;
   static constexpr int NU = NC + 1;      // conserved fields + temperature
-  static constexpr int MP = round_up(NP, 8);           // output rows, padded
-  static constexpr int MT = MP / 8;                    // m-tiles
+  static constexpr int MP = round_up(NP, T::MROW);     // output rows, padded
+  static constexpr int MT = MP / T::MROW;              // m-tiles
+  static constexpr int NAC = TF32 ? 2 : 1;             // A copies: tf32 hi/lo split
   static constexpr int NT = 256;                       // threads per CTA
-  // two resident CTAs per SM (<= 128 registers) unless the species make the
-  // pointwise flux state too large for that
-  static constexpr int MINB = (NC <= 7) ? 2 : 1;
+  // two resident CTAs per SM unless the species make the pointwise flux
+  // state too large for <= 128 registers
+  static constexpr int MINB = (NC <= 7 || TF32) ? 2 : 1;
   static constexpr int SMEM_BUDGET = 112 * 1024;
   static constexpr int GEO = DIM * DIM + NF * (DIM + 1);
 
   // gradient kernel operands: U [col][KU], face values [col][KS] with
   // col = field * EPB + element; matrices AW [DIM][MP][KU], AL [NF][MP][KL]
-  static constexpr int NFP4 = round_up(NFP, 4);
-  static constexpr int KU = mma_stride(NP);
-  static constexpr int KS = mma_stride(NF * NFP4);
-  static constexpr int KL = mma_stride(NFP4);
-  static constexpr int G_MAT = DIM * MP * KU + NF * MP * KL;
+  static constexpr int KUR = round_up(NP, T::KSTEP);     // k extent, volume
+  static constexpr int NFPK = round_up(NFP, T::KSTEP);   // k extent per face
+  static constexpr int KU = T::stride(KUR);
+  static constexpr int KS = T::stride(NF * NFPK);
+  static constexpr int KL = T::stride(NFPK);
+  static constexpr int G_MAT = NAC * (DIM * MP * KU + NF * MP * KL);
   static constexpr int G_PER_ELEM = NU * (KU + KS) + GEO;
-  static constexpr int EPB_G_RAW = (SMEM_BUDGET / 8 - G_MAT - 512) / G_PER_ELEM;
+  static constexpr int EPB_G_RAW = (SMEM_BUDGET / RB - G_MAT - 1024 / RB) / G_PER_ELEM;
   static constexpr int EPB_GRAD = imax(8, imin(32, EPB_G_RAW / 8 * 8));
   static constexpr int NCOL_G = round_up(NU * EPB_GRAD, 8);
 
   // rhs kernel operands: B [col][KB] = [G_0 .. G_{DIM-1} | S] per column,
   // A [MP][KB] = [-W_0 .. -W_{DIM-1} | LIFT]
   static constexpr int KR = DIM * NP + NFN;
-  static constexpr int KB = mma_stride(KR);
-  static constexpr int R_MAT = MP * KB;
+  static constexpr int KRR = round_up(KR, T::KSTEP);
+  static constexpr int KB = T::stride(KRR);
+  static constexpr int R_MAT = NAC * MP * KB;
   static constexpr int R_PER_ELEM = NC * KB + NC * NP + (MIX ? 2 * NP : 0) + NS * NP + GEO;
-  static constexpr int EPB_R_RAW = (SMEM_BUDGET / 8 - R_MAT - 512) / R_PER_ELEM;
+  static constexpr int EPB_R_RAW = (SMEM_BUDGET / RB - R_MAT - 1024 / RB) / R_PER_ELEM;
   static constexpr int EPB_RHS = imax(4, imin(32, EPB_R_RAW >= 8 ? EPB_R_RAW / 8 * 8
                                                                  : EPB_R_RAW / 4 * 4));
   static constexpr int NCOL_R = round_up(NC * EPB_RHS, 8);
 
   static size_t smem_grad(int nperm) {
-    return (size_t)(G_MAT + NCOL_G * (KU + KS) + EPB_GRAD * GEO) * 8 + NFN * 4 +
+    return (size_t)(G_MAT + NCOL_G * (KU + KS) + EPB_GRAD * GEO) * RB + NFN * 4 +
            (size_t)nperm * NFP + 64;
   }
   static size_t smem_rhs(int nperm) {
-    return (size_t)(R_MAT + NCOL_R * KB + EPB_RHS * (NC * NP + (MIX ? 2 * NP : 0) + NS * NP + GEO)) * 8 +
+    return (size_t)(R_MAT + NCOL_R * KB +
+                    EPB_RHS * (NC * NP + (MIX ? 2 * NP : 0) + NS * NP + GEO)) * RB +
            NFN * 4 + (size_t)nperm * NFP + 64;
   }
 };
@@ -124,6 +146,65 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
       "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
       : "+d"(d[0]), "+d"(d[1])
       : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// D(16x8) += A(16x8) * B(8x8) with tf32 operands, f32 accumulate.  Fragments
+// (g = lane/4, t = lane%4):  A: a0 A[g][t], a1 A[g+8][t], a2 A[g][t+4],
+// a3 A[g+8][t+4];  B: b0 B[t][g], b1 B[t+4][g];  D: d0 D[g][2t], d1 D[g][2t+1],
+// d2 D[g+8][2t], d3 D[g+8][2t+1].
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Three-term split product  A*B ~= Ahi*Bhi + Ahi*Blo + Alo*Bhi  on tf32
+// tensor cores; A arrives pre-split (hi/lo in shared memory), B is split here.
+__device__ __forceinline__ void mma_tf32x3(float (&d)[4], const uint32_t (&ahi)[4],
+                                           const uint32_t (&alo)[4], float b0, float b1) {
+  const uint32_t bh0 = to_tf32(b0), bh1 = to_tf32(b1);
+  const uint32_t bl0 = to_tf32(b0 - __uint_as_float(bh0));
+  const uint32_t bl1 = to_tf32(b1 - __uint_as_float(bh1));
+  mma_tf32(d, alo, bh0, bh1);
+  mma_tf32(d, ahi, bl0, bl1);
+  mma_tf32(d, ahi, bh0, bh1);
+}
+
+// hi/lo tf32 split of a float64 reference-matrix entry
+__device__ __forceinline__ void split_tf32(double v, float& hi, float& lo) {
+  hi = __uint_as_float(to_tf32((float)v));
+  lo = __uint_as_float(to_tf32((float)(v - (double)hi)));
+}
+
+// Store one reference-matrix entry into the A operand copies of type R.
+template <class R>
+__device__ __forceinline__ void put_a(R* a, int stride_copy, int i, double v) {
+  if constexpr (sizeof(R) == 8) {
+    a[i] = v;
+  } else {
+    float hi, lo;
+    split_tf32(v, hi, lo);
+    a[i] = hi;
+    a[stride_copy + i] = lo;
+  }
+}
+
+// A fragment (tf32) of rows m0.., k columns k0.. from a shared copy
+__device__ __forceinline__ void load_a_tf32(uint32_t (&a)[4], const float* am, int stride, int m0,
+                                            int k0, int g, int t) {
+  a[0] = __float_as_uint(am[(m0 + g) * stride + k0 + t]);
+  a[1] = __float_as_uint(am[(m0 + g + 8) * stride + k0 + t]);
+  a[2] = __float_as_uint(am[(m0 + g) * stride + k0 + t + 4]);
+  a[3] = __float_as_uint(am[(m0 + g + 8) * stride + k0 + t + 4]);
 }
 
 // Per-element geometry: rx copy, unit normals and face factors derived from rx
@@ -156,8 +237,9 @@ __device__ __forceinline__ void load_geometry(const R* __restrict__ rx_g, int e0
   }
 }
 
-// {{{ mixture temperature: T1 = Newton(seed), T2 = Newton(T1)
+// {{{ mixture temperature
 
+// plain form: T1 = Newton(seed), T2 = Newton(T1), fixed iteration count
 template <class R, int DIM, int NS>
 __global__ void __launch_bounds__(256) k_mixture_state(int64_t nnodes, const R* __restrict__ q,
                                                        const R* __restrict__ tseed,
@@ -175,25 +257,90 @@ __global__ void __launch_bounds__(256) k_mixture_state(int64_t nnodes, const R* 
   }
 }
 
+// mixed form: float32 Newton with an adaptive stop from the learned guess
+// (if given) else the seed; the float64 residual check
+//   |e(q) - e_mix(T)| / (c_v(T) T) <= rtol
+// accepts the result, otherwise the plain guess (seed) is iterated instead.
+// iters (optional) receives the float32 iteration count per node, with
+// 1000 added when the fallback ran; ST_NEWTON_MISS flags nodes that fail
+// both.
+template <int DIM, int NS>
+__global__ void __launch_bounds__(256) k_mixture_state_mixed(
+    int64_t nnodes, const float* __restrict__ q, const float* __restrict__ tseed,
+    const float* __restrict__ tguess, float* __restrict__ tout, int32_t* __restrict__ iters,
+    int maxit, float rtol, int32_t* status, GasParams g) {
+  constexpr int NC = DIM + 2 + NS;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  bool miss = false;
+  for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < nnodes; n += stride) {
+    float qq[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) qq[c] = q[(int64_t)c * nnodes + n];
+    float y[NS];
+    double yd[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      y[k] = qq[2 + DIM + k] / qq[0];
+      yd[k] = (double)qq[2 + DIM + k] / (double)qq[0];
+    }
+    double ked = 0;
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) ked += (double)qq[2 + i] * (double)qq[2 + i];
+    const double e64 = ((double)qq[1] - 0.5 * ked / (double)qq[0]) / (double)qq[0];
+    const float e32 = (float)e64;
+    int used = 0;
+    float t = 0.f;
+    bool ok = false;
+    // attempt 0: learned guess (when given); attempt 1: the plain guess (seed)
+    for (int attempt = tguess ? 0 : 1; attempt < 2 && !ok; ++attempt) {
+      t = (attempt == 0) ? tguess[n] : tseed[n];
+      for (int it = 0; it < maxit; ++it) {
+        float em, cv;
+        mixture_e_cv<float, NS>(y, t, em, cv);
+        const float dt = (e32 - em) / cv;
+        t += dt;
+        ++used;
+        if (fabsf(dt) <= rtol * 0.25f * fabsf(t)) break;
+      }
+      // float64 residual check; an accepted result takes the float64
+      // residual as one last Newton correction (float32 cannot resolve e(T)
+      // below ~1e-6 relative once formation enthalpies enter e)
+      double em, cv;
+      mixture_e_cv<double, NS>(yd, (double)t, em, cv);
+      const double corr = (e64 - em) / cv;
+      ok = t > 0.f && fabs(corr / (double)t) <= (double)rtol;
+      if (ok) t = (float)((double)t + corr);
+      if (!ok && attempt == 0) used += 1000;
+    }
+    if (!ok) miss = true;
+    tout[n] = t;
+    if (iters) iters[n] = used;
+  }
+  if (miss) atomicOr(status, ST_NEWTON_MISS);
+}
+
 // }}}
 
 // {{{ gradient kernel
 
-template <int DIM, int ORDER, int NS, bool MIX>
-__global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_grad(DGArgs<double> a, GasParams g) {
-  using C = Cfg<DIM, ORDER, NS, MIX>;
+template <class R, int DIM, int ORDER, int NS, bool MIX>
+__global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
+    k_grad(DGArgs<R> a, GasParams g) {
+  using C = Cfg<R, DIM, ORDER, NS, MIX>;
   using S = Simplex<DIM, ORDER>;
   constexpr int NP = C::NP, NF = C::NF, NFP = C::NFP, NFN = C::NFN, NC = C::NC, NU = C::NU;
-  constexpr int EPB = C::EPB_GRAD, MP = C::MP, MT = C::MT;
-  constexpr int KU = C::KU, KS = C::KS, KL = C::KL, NFP4 = C::NFP4, NCOL = C::NCOL_G;
+  constexpr int EPB = C::EPB_GRAD, MP = C::MP, MT = C::MT, NAC = C::NAC;
+  constexpr int KU = C::KU, KS = C::KS, KL = C::KL, NFPK = C::NFPK, NCOL = C::NCOL_G;
+  constexpr int KUR = C::KUR;
+  constexpr int AWN = DIM * MP * KU, ALN = NF * MP * KL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* aw = reinterpret_cast<double*>(smem_raw);        // [DIM][MP][KU]
-  double* al = aw + DIM * MP * KU;                         // [NF][MP][KL]
-  double* bu = al + NF * MP * KL;                          // [NCOL][KU]
-  double* bs = bu + NCOL * KU;                              // [NCOL][KS]
-  double* rx_s = bs + NCOL * KS;                           // [EPB][DIM][DIM]
-  double* nrm_s = rx_s + EPB * DIM * DIM;                  // [EPB][NF][DIM]
-  double* fs_s = nrm_s + EPB * NF * DIM;                   // [EPB][NF]
+  R* aw = reinterpret_cast<R*>(smem_raw);                  // [NAC][DIM][MP][KU]
+  R* al = aw + NAC * AWN;                                  // [NAC][NF][MP][KL]
+  R* bu = al + NAC * ALN;                                  // [NCOL][KU]
+  R* bs = bu + NCOL * KU;                                  // [NCOL][KS]
+  R* rx_s = bs + NCOL * KS;                                // [EPB][DIM][DIM]
+  R* nrm_s = rx_s + EPB * DIM * DIM;                       // [EPB][NF][DIM]
+  R* fs_s = nrm_s + EPB * NF * DIM;                        // [EPB][NF]
   int* fn_s = reinterpret_cast<int*>(fs_s + EPB * NF);     // [NF*NFP]
   uint8_t* perm_s = reinterpret_cast<uint8_t*>(fn_s + NFN);
 
@@ -202,51 +349,43 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_grad(
   const int ne = imin(EPB, E - e0);
   const int64_t EN = (int64_t)E * NP;
 
-  // reference operators (zero padded) and zeroed operand tiles
-  for (int i = threadIdx.x; i < DIM * MP * KU; i += blockDim.x) {
+  // reference operators (zero padded; hi/lo tf32 split on the mixed path)
+  for (int i = threadIdx.x; i < AWN; i += blockDim.x) {
     const int r = i / (MP * KU), row = (i / KU) % MP, k = i % KU;
-    aw[i] = (row < NP && k < NP) ? c_ref64[S::OFF_W + (r * NP + row) * NP + k] : 0.0;
+    put_a<R>(aw, AWN, i, (row < NP && k < NP) ? c_ref64[S::OFF_W + (r * NP + row) * NP + k] : 0.0);
   }
-  for (int i = threadIdx.x; i < NF * MP * KL; i += blockDim.x) {
+  for (int i = threadIdx.x; i < ALN; i += blockDim.x) {
     const int f = i / (MP * KL), row = (i / KL) % MP, m = i % KL;
-    al[i] = (row < NP && m < NFP) ? c_ref64[S::OFF_LIFT + row * NFN + f * NFP + m] : 0.0;
+    put_a<R>(al, ALN, i,
+             (row < NP && m < NFP) ? c_ref64[S::OFF_LIFT + row * NFN + f * NFP + m] : 0.0);
   }
-  for (int i = threadIdx.x; i < NCOL * (KU + KS); i += blockDim.x) bu[i] = 0.0;
+  for (int i = threadIdx.x; i < NCOL * (KU + KS); i += blockDim.x) bu[i] = R(0);
   for (int i = threadIdx.x; i < NFN; i += blockDim.x) fn_s[i] = c_face_nodes<DIM, ORDER>(i);
   for (int i = threadIdx.x; i < a.nperm * NFP; i += blockDim.x) perm_s[i] = a.perm[i];
-  load_geometry<double, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);   // syncs once
+  load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);   // syncs once
   __syncthreads();
 
-  // phase 1: conserved fields (and temperature) of the tile into U
-  for (int c = 0; c < NC; ++c)
-    for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
-      const int e = idx / NP, k = idx % NP;
-      bu[(c * EPB + e) * KU + k] = a.q[c * EN + (int64_t)e0 * NP + idx];
-    }
-  if (MIX)
-    for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
-      const int e = idx / NP, k = idx % NP;
-      bu[(NC * EPB + e) * KU + k] = a.t_op[(int64_t)e0 * NP + idx];
-    }
-  __syncthreads();
-  if (!MIX) {
-    for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
-      const int e = idx / NP, k = idx % NP;
-      double qq[NC];
+  // phase 1: conserved fields and temperature of the tile into U
+  for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
+    const int e = idx / NP, k = idx % NP;
+    R qq[NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) qq[c] = bu[(c * EPB + e) * KU + k];
-      bu[(NC * EPB + e) * KU + k] = node_temperature<double, DIM, NS>(qq, 0.0, g);
+    for (int c = 0; c < NC; ++c) {
+      qq[c] = a.q[c * EN + (int64_t)e0 * NP + idx];
+      bu[(c * EPB + e) * KU + k] = qq[c];
     }
-    __syncthreads();
+    bu[(NC * EPB + e) * KU + k] =
+        MIX ? a.t_op[(int64_t)e0 * NP + idx] : node_temperature<R, DIM, NS>(qq, R(0), g);
   }
+  __syncthreads();
 
   // phase 3: face values  fscale * u*   (u* = central average or boundary value)
   for (int idx = threadIdx.x; idx < ne * NFN; idx += blockDim.x) {
     const int e = idx / NFN, fm = idx % NFN, f = fm / NFP, m = fm % NFP;
     const int k = fn_s[fm];
     const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
-    const double fsc = fs_s[e * NF + f];
-    double up[NU];
+    const R fsc = fs_s[e * NF + f];
+    R up[NU];
     bool central = true;
     if (cn >= 0) {
       const int en = cn >> 8, pr = cn & 255;
@@ -259,7 +398,7 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_grad(
         const int64_t gi = (int64_t)en * NP + kn;
 #pragma unroll
         for (int c = 0; c < NC; ++c) up[c] = a.q[c * EN + gi];
-        up[NC] = MIX ? a.t_op[gi] : node_temperature<double, DIM, NS>(up, 0.0, g);
+        up[NC] = MIX ? a.t_op[gi] : node_temperature<R, DIM, NS>(up, R(0), g);
       }
     } else {
       const int bf = -(cn + 1);
@@ -269,7 +408,7 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_grad(
 #pragma unroll
         for (int c = 0; c < NC; ++c) up[c] = a.bext[c * bstride + (int64_t)bf * NFP + m];
         up[NC] = MIX ? a.bext[NC * bstride + (int64_t)bf * NFP + m]
-                     : node_temperature<double, DIM, NS>(up, 0.0, g);
+                     : node_temperature<R, DIM, NS>(up, R(0), g);
         central = false;   // the gradient flux sends the exterior value
       } else {
         if (kind < 0) atomicOr(a.status, ST_BAD_INDEX);
@@ -279,54 +418,98 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_grad(
     }
 #pragma unroll
     for (int c = 0; c < NU; ++c) {
-      const double um = bu[(c * EPB + e) * KU + k];
-      const double ustar = central ? (up[c] + um) / 2 : up[c];
-      bs[(c * EPB + e) * KS + f * NFP4 + m] = fsc * ustar;
+      const R um = bu[(c * EPB + e) * KU + k];
+      const R ustar = central ? (up[c] + um) / R(2) : up[c];
+      // element-constant shift (node 0 value): the discrete gradient of a
+      // constant vanishes, so subtracting it changes nothing in exact
+      // arithmetic and keeps large means out of the contraction
+      bs[(c * EPB + e) * KS + f * NFPK + m] = fsc * (ustar - bu[(c * EPB + e) * KU]);
     }
   }
   __syncthreads();
+  for (int p = threadIdx.x; p < NU * ne; p += blockDim.x) {
+    const int c = p / ne, e = p % ne;
+    R* row = bu + (c * EPB + e) * KU;
+    const R u0 = row[0];
+#pragma unroll 4
+    for (int k = 0; k < NP; ++k) row[k] -= u0;
+  }
+  __syncthreads();
 
-  // phase 4: per 8-column tile, du_r = W_r U and L_f = LIFT_f S on the
-  // float64 tensor cores, then grad_j = sum_f n_fj L_f - sum_r rx_rj du_r
+  // phase 4: per 8-column tile, du_r = W_r U and L_f = LIFT_f S on the tensor
+  // cores, then grad_j = sum_f n_fj L_f - sum_r rx_rj du_r
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gq = lane >> 2, tq = lane & 3;
+  constexpr int NACC = C::TF32 ? 4 : 2;     // accumulator entries per lane per m-tile
   for (int nt = warp; nt < NCOL / 8; nt += blockDim.x >> 5) {
-    double du[DIM][MT][2], lf[NF][MT][2];
+    R du[DIM][MT][NACC], lf[NF][MT][NACC];
 #pragma unroll
     for (int r = 0; r < DIM; ++r)
 #pragma unroll
-      for (int t = 0; t < MT; ++t) du[r][t][0] = du[r][t][1] = 0.0;
+      for (int t = 0; t < MT; ++t)
+#pragma unroll
+        for (int v = 0; v < NACC; ++v) du[r][t][v] = R(0);
 #pragma unroll
     for (int f = 0; f < NF; ++f)
 #pragma unroll
-      for (int t = 0; t < MT; ++t) lf[f][t][0] = lf[f][t][1] = 0.0;
-    const double* bcol = bu + (nt * 8 + gq) * KU + tq;
+      for (int t = 0; t < MT; ++t)
 #pragma unroll
-    for (int ks = 0; ks < KU / 4; ++ks) {
-      if (ks * 4 >= NP) break;
-      const double b = bcol[ks * 4];
+        for (int v = 0; v < NACC; ++v) lf[f][t][v] = R(0);
+    const R* bcol = bu + (nt * 8 + gq) * KU + tq;
+    const R* scol = bs + (nt * 8 + gq) * KS + tq;
+    if constexpr (!C::TF32) {
 #pragma unroll
-      for (int r = 0; r < DIM; ++r)
+      for (int ks = 0; ks < KUR / 4; ++ks) {
+        const double b = bcol[ks * 4];
 #pragma unroll
-        for (int t = 0; t < MT; ++t)
-          dmma884(du[r][t], aw[(r * MP + t * 8 + gq) * KU + ks * 4 + tq], b);
-    }
-    const double* scol = bs + (nt * 8 + gq) * KS + tq;
+        for (int r = 0; r < DIM; ++r)
 #pragma unroll
-    for (int f = 0; f < NF; ++f)
-#pragma unroll
-      for (int ks = 0; ks < NFP4 / 4; ++ks) {
-        const double b = scol[f * NFP4 + ks * 4];
-#pragma unroll
-        for (int t = 0; t < MT; ++t)
-          dmma884(lf[f][t], al[(f * MP + t * 8 + gq) * KL + ks * 4 + tq], b);
+          for (int t = 0; t < MT; ++t)
+            dmma884(du[r][t], aw[(r * MP + t * 8 + gq) * KU + ks * 4 + tq], b);
       }
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int ks = 0; ks < NFPK / 4; ++ks) {
+          const double b = scol[f * NFPK + ks * 4];
+#pragma unroll
+          for (int t = 0; t < MT; ++t)
+            dmma884(lf[f][t], al[(f * MP + t * 8 + gq) * KL + ks * 4 + tq], b);
+        }
+    } else {
+#pragma unroll
+      for (int ks = 0; ks < KUR / 8; ++ks) {
+        const float b0 = bcol[ks * 8], b1 = bcol[ks * 8 + 4];
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+          for (int t = 0; t < MT; ++t) {
+            uint32_t ah[4], alo[4];
+            load_a_tf32(ah, aw + r * MP * KU, KU, t * 16, ks * 8, gq, tq);
+            load_a_tf32(alo, aw + AWN + r * MP * KU, KU, t * 16, ks * 8, gq, tq);
+            mma_tf32x3(du[r][t], ah, alo, b0, b1);
+          }
+      }
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int ks = 0; ks < NFPK / 8; ++ks) {
+          const float b0 = scol[f * NFPK + ks * 8], b1 = scol[f * NFPK + ks * 8 + 4];
+#pragma unroll
+          for (int t = 0; t < MT; ++t) {
+            uint32_t ah[4], alo[4];
+            load_a_tf32(ah, al + f * MP * KL, KL, t * 16, ks * 8, gq, tq);
+            load_a_tf32(alo, al + ALN + f * MP * KL, KL, t * 16, ks * 8, gq, tq);
+            mma_tf32x3(lf[f][t], ah, alo, b0, b1);
+          }
+        }
+    }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int col = nt * 8 + 2 * tq + h;
       const int c = col / EPB, e = col % EPB;
       if (c >= NU || e >= ne) continue;
-      double rxe[DIM][DIM], nre[NF][DIM];
+      R rxe[DIM][DIM], nre[NF][DIM];
 #pragma unroll
       for (int r = 0; r < DIM; ++r)
 #pragma unroll
@@ -335,21 +518,24 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_grad(
       for (int f = 0; f < NF; ++f)
 #pragma unroll
         for (int j = 0; j < DIM; ++j) nre[f][j] = nrm_s[(e * NF + f) * DIM + j];
-      double* outp = a.out + ((int64_t)c * DIM) * EN + (int64_t)(e0 + e) * NP;
+      R* outp = a.out + ((int64_t)c * DIM) * EN + (int64_t)(e0 + e) * NP;
 #pragma unroll
-      for (int t = 0; t < MT; ++t) {
-        const int i = t * 8 + gq;
-        if (i >= NP) continue;
+      for (int t = 0; t < MT; ++t)
 #pragma unroll
-        for (int j = 0; j < DIM; ++j) {
-          double gsum = 0.0;
+        for (int half = 0; half < NACC / 2; ++half) {
+          const int i = t * Tile<R>::MROW + gq + 8 * half;
+          if (i >= NP) continue;
+          const int v = 2 * half + h;
 #pragma unroll
-          for (int f = 0; f < NF; ++f) gsum += nre[f][j] * lf[f][t][h];
+          for (int j = 0; j < DIM; ++j) {
+            R gsum = R(0);
 #pragma unroll
-          for (int r = 0; r < DIM; ++r) gsum -= rxe[r][j] * du[r][t][h];
-          outp[(int64_t)j * EN + i] = gsum;
+            for (int f = 0; f < NF; ++f) gsum += nre[f][j] * lf[f][t][v];
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) gsum -= rxe[r][j] * du[r][t][v];
+            outp[(int64_t)j * EN + i] = gsum;
+          }
         }
-      }
     }
   }
 }
@@ -358,22 +544,23 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_grad(
 
 // {{{ rhs kernel (Euler when VISC is false)
 
-template <int DIM, int ORDER, int NS, bool MIX, bool VISC>
-__global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_rhs(DGArgs<double> a, GasParams g) {
-  using C = Cfg<DIM, ORDER, NS, MIX>;
+template <class R, int DIM, int ORDER, int NS, bool MIX, bool VISC>
+__global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
+    k_rhs(DGArgs<R> a, GasParams g) {
+  using C = Cfg<R, DIM, ORDER, NS, MIX>;
   using S = Simplex<DIM, ORDER>;
   constexpr int NP = C::NP, NF = C::NF, NFP = C::NFP, NFN = C::NFN, NC = C::NC;
   constexpr int EPB = C::EPB_RHS, MP = C::MP, MT = C::MT, KB = C::KB, KR = C::KR;
-  constexpr int NCOL = C::NCOL_R;
+  constexpr int KRR = C::KRR, NCOL = C::NCOL_R, NAC = C::NAC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* am = reinterpret_cast<double*>(smem_raw);        // [MP][KB]
-  double* bm = am + MP * KB;                               // [NCOL][KB]
-  double* q_s = bm + NCOL * KB;                            // [NC][EPB][NP]
-  double* t_s = q_s + NC * EPB * NP;                       // [2][EPB][NP] (MIX)
-  double* src_s = t_s + (MIX ? 2 * EPB * NP : 0);          // [NS][EPB][NP] (MIX)
-  double* rx_s = src_s + NS * EPB * NP;                    // [EPB][DIM][DIM]
-  double* nrm_s = rx_s + EPB * DIM * DIM;
-  double* fs_s = nrm_s + EPB * NF * DIM;
+  R* am = reinterpret_cast<R*>(smem_raw);                  // [NAC][MP][KB]
+  R* bm = am + NAC * MP * KB;                              // [NCOL][KB]
+  R* q_s = bm + NCOL * KB;                                 // [NC][EPB][NP]
+  R* t_s = q_s + NC * EPB * NP;                            // [2][EPB][NP] (MIX)
+  R* src_s = t_s + (MIX ? 2 * EPB * NP : 0);               // [NS][EPB][NP] (MIX)
+  R* rx_s = src_s + NS * EPB * NP;                         // [EPB][DIM][DIM]
+  R* nrm_s = rx_s + EPB * DIM * DIM;
+  R* fs_s = nrm_s + EPB * NF * DIM;
   int* fn_s = reinterpret_cast<int*>(fs_s + EPB * NF);
   uint8_t* perm_s = reinterpret_cast<uint8_t*>(fn_s + NFN);
 
@@ -395,9 +582,9 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_rhs(D
         v = c_ref64[S::OFF_LIFT + row * NFN + (k - DIM * NP)];
       }
     }
-    am[i] = v;
+    put_a<R>(am, MP * KB, i, v);
   }
-  for (int i = threadIdx.x; i < NCOL * KB; i += blockDim.x) bm[i] = 0.0;
+  for (int i = threadIdx.x; i < NCOL * KB; i += blockDim.x) bm[i] = R(0);
   for (int i = threadIdx.x; i < NFN; i += blockDim.x) fn_s[i] = c_face_nodes<DIM, ORDER>(i);
   for (int i = threadIdx.x; i < a.nperm * NFP; i += blockDim.x) perm_s[i] = a.perm[i];
   for (int c = 0; c < NC; ++c)
@@ -406,36 +593,36 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_rhs(D
   if (MIX)
     for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
       t_s[idx] = a.t_op[(int64_t)e0 * NP + idx];
-      t_s[EPB * NP + idx] = sources ? a.t_src[(int64_t)e0 * NP + idx] : 0.0;
+      t_s[EPB * NP + idx] = sources ? a.t_src[(int64_t)e0 * NP + idx] : R(0);
     }
-  load_geometry<double, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
+  load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
   __syncthreads();
 
   // phase 2: volume flux F = F_V - F_I, metric-combined into B[col][r*NP + k]
   for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
     const int e = idx / NP, k = idx % NP;
-    double qq[NC];
+    R qq[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) qq[c] = q_s[(c * EPB) * NP + idx];
-    NodeState<double, DIM, NS> st;
-    make_state<double, DIM, NS>(qq, MIX ? t_s[idx] : 0.0, g, st);
-    double fl[NC][DIM];
-    inviscid_flux<double, DIM, NS>(st, fl);
+    NodeState<R, DIM, NS> st;
+    make_state<R, DIM, NS>(qq, MIX ? t_s[idx] : R(0), g, st);
+    R fl[NC][DIM];
+    inviscid_flux<R, DIM, NS>(st, fl);
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
       for (int j = 0; j < DIM; ++j) fl[c][j] = -fl[c][j];
     if (VISC) {
-      double gq[NC][DIM], gt[DIM];
+      R gqv[NC][DIM], gt[DIM];
       const int64_t gi = (int64_t)e0 * NP + idx;
 #pragma unroll
       for (int c = 0; c < NC; ++c)
 #pragma unroll
-        for (int j = 0; j < DIM; ++j) gq[c][j] = a.grad[((int64_t)c * DIM + j) * EN + gi];
+        for (int j = 0; j < DIM; ++j) gqv[c][j] = a.grad[((int64_t)c * DIM + j) * EN + gi];
 #pragma unroll
       for (int j = 0; j < DIM; ++j) gt[j] = a.grad[((int64_t)NC * DIM + j) * EN + gi];
-      double fv[NC][DIM];
-      viscous_flux<double, DIM, NS, MIX>(st, gq, gt, fv);
+      R fv[NC][DIM];
+      viscous_flux<R, DIM, NS, MIX>(st, gqv, gt, fv);
 #pragma unroll
       for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -445,17 +632,23 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_rhs(D
     for (int c = 0; c < NC; ++c)
 #pragma unroll
       for (int r = 0; r < DIM; ++r) {
-        double acc = 0.0;
+        R acc = R(0);
 #pragma unroll
         for (int j = 0; j < DIM; ++j) acc += rx_s[e * DIM * DIM + r * DIM + j] * fl[c][j];
         bm[(c * EPB + e) * KB + r * NP + k] = acc;
       }
     if constexpr (MIX && NS > 0) {
       if (sources) {
-        double om[NS];
-        production_rates<double, NS>(st.rho, t_s[EPB * NP + idx], st.y, g.zero_level, om);
+        // Arrhenius sources in float64 on both paths: near-equilibrium
+        // forward/reverse cancellation and exp(-Ta/T) would amplify float32
+        // rounding (the mixed form keeps only flux/EOS math in float32)
+        double om[NS], yd[NS];
+        const double rhod = (double)qq[0];
 #pragma unroll
-        for (int s = 0; s < NS; ++s) src_s[(s * EPB) * NP + idx] = c_mech.mw[s] * om[s];
+        for (int s = 0; s < NS; ++s) yd[s] = (double)qq[2 + DIM + s] / rhod;
+        production_rates<double, NS>(rhod, (double)t_s[EPB * NP + idx], yd, g.zero_level, om);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) src_s[(s * EPB) * NP + idx] = (R)(c_mech.mw[s] * om[s]);
       }
     }
   }
@@ -466,35 +659,39 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_rhs(D
     const int e = idx / NFN, fm = idx % NFN, f = fm / NFP, m = fm % NFP;
     const int k = fn_s[fm];
     const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
-    const double fsc = fs_s[e * NF + f];
-    double n[DIM];
+    const R fsc = fs_s[e * NF + f];
+    R n[DIM];
 #pragma unroll
     for (int j = 0; j < DIM; ++j) n[j] = nrm_s[(e * NF + f) * DIM + j];
-    double qm[NC], qp[NC];
+    R qm[NC], qp[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) qm[c] = q_s[(c * EPB + e) * NP + k];
-    NodeState<double, DIM, NS> sm, sp;
-    make_state<double, DIM, NS>(qm, MIX ? t_s[e * NP + k] : 0.0, g, sm);
+    NodeState<R, DIM, NS> sm, sp;
+    make_state<R, DIM, NS>(qm, MIX ? t_s[e * NP + k] : R(0), g, sm);
     // own total flux . n from the metric-combined volume flux:
     // F.n = (sum_r N_r G_r) / |rx^T N|
-    double nmag2 = 0.0;
+    R nmag2 = R(0);
 #pragma unroll
     for (int j = 0; j < DIM; ++j) {
-      double a2 = 0.0;
+      R a2 = R(0);
 #pragma unroll
       for (int r = 0; r < DIM; ++r)
-        a2 += rx_s[e * DIM * DIM + r * DIM + j] * c_ref64[S::OFF_NREF + f * DIM + r];
+        a2 += rx_s[e * DIM * DIM + r * DIM + j] * RefBank<R>::get(S::OFF_NREF + f * DIM + r);
       nmag2 += a2 * a2;
     }
-    const double inmag = 1.0 / sqrt(nmag2);
-    double ftm[NC];
+    const R inmag = R(1) / sqrt(nmag2);
+    R ftm[NC], f0n[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      double acc = 0.0;
+      R acc = R(0), acc0 = R(0);
 #pragma unroll
-      for (int r = 0; r < DIM; ++r)
-        acc += c_ref64[S::OFF_NREF + f * DIM + r] * bm[(c * EPB + e) * KB + r * NP + k];
+      for (int r = 0; r < DIM; ++r) {
+        const R nr = RefBank<R>::get(S::OFF_NREF + f * DIM + r);
+        acc += nr * bm[(c * EPB + e) * KB + r * NP + k];
+        acc0 += nr * bm[(c * EPB + e) * KB + r * NP];
+      }
       ftm[c] = acc * inmag;
+      f0n[c] = acc0 * inmag;     // element-constant shift: node-0 flux . n
     }
     int mode = 0;   // 0 interior, 1 dummy (interior only), 2 prescribed exterior
     int64_t gi = 0;
@@ -508,7 +705,7 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_rhs(D
         gi = (int64_t)en * NP + kn;
 #pragma unroll
         for (int c = 0; c < NC; ++c) qp[c] = a.q[c * EN + gi];
-        make_state<double, DIM, NS>(qp, MIX ? a.t_op[gi] : 0.0, g, sp);
+        make_state<R, DIM, NS>(qp, MIX ? a.t_op[gi] : R(0), g, sp);
       }
     } else {
       const int bf = -(cn + 1);
@@ -518,28 +715,28 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_rhs(D
         const int64_t bstride = (int64_t)a.nbf * NFP;
 #pragma unroll
         for (int c = 0; c < NC; ++c) qp[c] = a.bext[c * bstride + (int64_t)bf * NFP + m];
-        make_state<double, DIM, NS>(qp, MIX ? a.bext[NC * bstride + (int64_t)bf * NFP + m] : 0.0,
-                                    g, sp);
+        make_state<R, DIM, NS>(qp, MIX ? a.bext[NC * bstride + (int64_t)bf * NFP + m] : R(0),
+                               g, sp);
       } else {
         if (kind < 0) atomicOr(a.status, ST_BAD_INDEX);
         mode = 1;
       }
     }
-    double out[NC];
+    R out[NC];
     if (mode == 1) {
       // DummyBoundary: F_V(q-).n - F_I(q-).n  (boundary.py:1027-1049)
 #pragma unroll
       for (int c = 0; c < NC; ++c) out[c] = ftm[c];
     } else {
-      double fi[NC];
-      inviscid_num_flux<double, DIM, NS>(sm, sp, qm, qp, n, a.flux_kind, fi);
+      R fi[NC];
+      inviscid_num_flux<R, DIM, NS>(sm, sp, qm, qp, n, a.flux_kind, fi);
 #pragma unroll
       for (int c = 0; c < NC; ++c) out[c] = -fi[c];
       if (VISC) {
         // own viscous part: F_V- . n = (F_V - F_I)- . n + F_I- . n
-        double fim[NC];
-        inviscid_flux_n<double, DIM, NS>(sm, n, fim);
-        double gqp[NC][DIM], gtp[DIM];
+        R fim[NC];
+        inviscid_flux_n<R, DIM, NS>(sm, n, fim);
+        R gqp[NC][DIM], gtp[DIM];
         const int64_t gsrc = (mode == 0) ? gi : (int64_t)(e0 + e) * NP + k;
 #pragma unroll
         for (int c = 0; c < NC; ++c)
@@ -547,53 +744,82 @@ __global__ void __launch_bounds__(256, (Cfg<DIM, ORDER, NS, MIX>::MINB)) k_rhs(D
           for (int j = 0; j < DIM; ++j) gqp[c][j] = a.grad[((int64_t)c * DIM + j) * EN + gsrc];
 #pragma unroll
         for (int j = 0; j < DIM; ++j) gtp[j] = a.grad[((int64_t)NC * DIM + j) * EN + gsrc];
-        double fvp[NC][DIM];
-        viscous_flux<double, DIM, NS, MIX>(sp, gqp, gtp, fvp);
+        R fvp[NC][DIM];
+        viscous_flux<R, DIM, NS, MIX>(sp, gqp, gtp, fvp);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          double fvpn = 0.0;
+          R fvpn = R(0);
 #pragma unroll
           for (int j = 0; j < DIM; ++j) fvpn += fvp[c][j] * n[j];
-          const double fvmn = ftm[c] + fim[c];
-          out[c] += (fvmn + fvpn) / 2;
+          const R fvmn = ftm[c] + fim[c];
+          out[c] += (fvmn + fvpn) / R(2);
         }
       }
     }
 #pragma unroll
-    for (int c = 0; c < NC; ++c) bm[(c * EPB + e) * KB + DIM * NP + fm] = fsc * out[c];
+    for (int c = 0; c < NC; ++c) bm[(c * EPB + e) * KB + DIM * NP + fm] = fsc * (out[c] - f0n[c]);
+  }
+  __syncthreads();
+  // subtract the node-0 flux from the volume terms: with the face terms
+  // shifted by F0 . n above, the divergence is unchanged in exact arithmetic
+  for (int p = threadIdx.x; p < NC * ne * DIM; p += blockDim.x) {
+    const int r = p % DIM, ce = p / DIM, c = ce / ne, e = ce % ne;
+    R* row = bm + (c * EPB + e) * KB + r * NP;
+    const R g0 = row[0];
+#pragma unroll 4
+    for (int k = 0; k < NP; ++k) row[k] -= g0;
   }
   __syncthreads();
 
-  // phase 4: rhs = [-W | LIFT] [G ; S] on the float64 tensor cores (+ sources)
+  // phase 4: rhs = [-W | LIFT] [G ; S] on the tensor cores (+ sources)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gq = lane >> 2, tq = lane & 3;
+  constexpr int NACC = C::TF32 ? 4 : 2;
   bool bad = false;
   for (int nt = warp; nt < NCOL / 8; nt += blockDim.x >> 5) {
-    double d[MT][2];
+    R d[MT][NACC];
 #pragma unroll
-    for (int t = 0; t < MT; ++t) d[t][0] = d[t][1] = 0.0;
-    const double* bcol = bm + (nt * 8 + gq) * KB + tq;
+    for (int t = 0; t < MT; ++t)
+#pragma unroll
+      for (int v = 0; v < NACC; ++v) d[t][v] = R(0);
+    const R* bcol = bm + (nt * 8 + gq) * KB + tq;
+    if constexpr (!C::TF32) {
 #pragma unroll 5
-    for (int ks = 0; ks < (KR + 3) / 4; ++ks) {
-      const double b = bcol[ks * 4];
+      for (int ks = 0; ks < KRR / 4; ++ks) {
+        const double b = bcol[ks * 4];
 #pragma unroll
-      for (int t = 0; t < MT; ++t) dmma884(d[t], am[(t * 8 + gq) * KB + ks * 4 + tq], b);
+        for (int t = 0; t < MT; ++t) dmma884(d[t], am[(t * 8 + gq) * KB + ks * 4 + tq], b);
+      }
+    } else {
+#pragma unroll 2
+      for (int ks = 0; ks < KRR / 8; ++ks) {
+        const float b0 = bcol[ks * 8], b1 = bcol[ks * 8 + 4];
+#pragma unroll
+        for (int t = 0; t < MT; ++t) {
+          uint32_t ah[4], alo[4];
+          load_a_tf32(ah, am, KB, t * 16, ks * 8, gq, tq);
+          load_a_tf32(alo, am + MP * KB, KB, t * 16, ks * 8, gq, tq);
+          mma_tf32x3(d[t], ah, alo, b0, b1);
+        }
+      }
     }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int col = nt * 8 + 2 * tq + h;
       const int c = col / EPB, e = col % EPB;
       if (c >= NC || e >= ne) continue;
-      double* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
+      R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
 #pragma unroll
-      for (int t = 0; t < MT; ++t) {
-        const int i = t * 8 + gq;
-        if (i >= NP) continue;
-        double v = d[t][h];
-        if (sources && c >= 2 + DIM) v += src_s[((c - 2 - DIM) * EPB + e) * NP + i];
-        outp[i] = v;
-        bad |= !(v == v);
-      }
+      for (int t = 0; t < MT; ++t)
+#pragma unroll
+        for (int half = 0; half < NACC / 2; ++half) {
+          const int i = t * Tile<R>::MROW + gq + 8 * half;
+          if (i >= NP) continue;
+          R v = d[t][2 * half + h];
+          if (sources && c >= 2 + DIM) v += src_s[((c - 2 - DIM) * EPB + e) * NP + i];
+          outp[i] = v;
+          bad |= !(v == v);
+        }
     }
   }
   if (bad) atomicOr(a.status, ST_NAN);
@@ -629,6 +855,33 @@ __global__ void k_rk4_stage(int64_t n, const double* __restrict__ q0, const doub
     }
     qout[i] = qn;
     if (qout_lo) qout_lo[i] = (R)qn;
+  }
+}
+
+// mixed form: k arrives in float32, the state and the sum stay float64, and
+// the float32 copy of the new state feeds the next right-hand side
+static __global__ void k_rk4_stage_mixed(int64_t n, const double* __restrict__ q0,
+                                  const float* __restrict__ k, double* __restrict__ sum,
+                                  double* __restrict__ qout, float* __restrict__ qout_lo,
+                                  int stage, double dt) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double kv = (double)k[i];
+    double qn;
+    if (stage == 0) {
+      sum[i] = kv;
+      qn = q0[i] + dt / 2 * kv;
+    } else if (stage == 1) {
+      sum[i] = sum[i] + 2.0 * kv;
+      qn = q0[i] + dt / 2 * kv;
+    } else if (stage == 2) {
+      sum[i] = sum[i] + 2.0 * kv;
+      qn = q0[i] + dt * kv;
+    } else {
+      qn = q0[i] + dt / 6 * (sum[i] + kv);
+    }
+    qout[i] = qn;
+    qout_lo[i] = (float)qn;
   }
 }
 

@@ -15,6 +15,16 @@ int tu2_dispatch(int, int, int, bool, const DGArgs<double>&, const GasParams&, c
 int tu3_dispatch(int, int, int, bool, const DGArgs<double>&, const GasParams&, cudaStream_t);
 int tu2_mixture_state(int, int64_t, const double*, const double*, double*, double*,
                       const GasParams&, cudaStream_t);
+int tu2f_upload_refops(int, int, const double*, const float*, const int*);
+int tu3f_upload_refops(int, int, const double*, const float*, const int*);
+int tu2f_upload_mechanism(const Mechanism*);
+int tu3f_upload_mechanism(const Mechanism*);
+int tu2f_dispatch(int, int, int, bool, const DGArgs<float>&, const GasParams&, cudaStream_t);
+int tu3f_dispatch(int, int, int, bool, const DGArgs<float>&, const GasParams&, cudaStream_t);
+int tu2f_mixture_state(int, int64_t, const float*, const float*, const float*, float*, int32_t*,
+                       int, float, int32_t*, const GasParams&, cudaStream_t);
+int tu3f_mixture_state(int, int64_t, const float*, const float*, const float*, float*, int32_t*,
+                       int, float, int32_t*, const GasParams&, cudaStream_t);
 int tu3_mixture_state(int, int64_t, const double*, const double*, double*, double*,
                       const GasParams&, cudaStream_t);
 }  // namespace mgc
@@ -55,10 +65,11 @@ int ready(const mgc_mesh_t* m, const mgc_gas_t* g) {
   return MGC_OK;
 }
 
-DGArgs<double> make_args(const mgc_mesh_t* m, const double* q, const double* t_op,
-                         const double* t_src, const double* grad, double* out,
-                         const double* bext, int flux_kind, int add_sources, int32_t* status) {
-  DGArgs<double> a;
+template <class R>
+DGArgs<R> make_args(const mgc_mesh_t* m, const R* q, const R* t_op, const R* t_src,
+                    const R* grad, R* out, const R* bext, int flux_kind, int add_sources,
+                    int32_t* status) {
+  DGArgs<R> a;
   std::memset(&a, 0, sizeof(a));
   a.nelem = m->nelem;
   a.nbf = m->nbf;
@@ -69,7 +80,11 @@ DGArgs<double> make_args(const mgc_mesh_t* m, const double* q, const double* t_o
   a.t_src = t_src;
   a.grad = grad;
   a.out = out;
-  a.rx = m->rx;
+  if constexpr (sizeof(R) == 8) {
+    a.rx = m->rx;
+  } else {
+    a.rx = m->rx32;
+  }
   a.conn = m->conn;
   a.perm = m->perm;
   a.bkind = m->bkind;
@@ -92,6 +107,55 @@ int dispatch(int op, const mgc_mesh_t* m, const mgc_gas_t* g, const DGArgs<doubl
   const GasParams p = to_params(g);
   if (m->dim == 2) return tu2_dispatch(op, m->order, g->nspecies, mix, a, p, s);
   return tu3_dispatch(op, m->order, g->nspecies, mix, a, p, s);
+}
+
+int dispatch(int op, const mgc_mesh_t* m, const mgc_gas_t* g, const DGArgs<float>& a,
+             cudaStream_t s) {
+  const bool mix = g->eos_kind == MGC_EOS_MIXTURE;
+  if (!supported_species_f32(g->nspecies, mix)) return MGC_E_UNSUPPORTED;
+  if (!m->rx32) return MGC_E_INVALID;
+  const GasParams p = to_params(g);
+  if (m->dim == 2) return tu2f_dispatch(op, m->order, g->nspecies, mix, a, p, s);
+  return tu3f_dispatch(op, m->order, g->nspecies, mix, a, p, s);
+}
+
+template <class R>
+int euler_rhs_impl(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const R* q, const R* t_op,
+                   const R* bext, int flux_kind, R* rhs, int32_t* status, void* stream) {
+  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !rhs || !status) return MGC_E_INVALID;
+  if (flux_kind < 0 || flux_kind > 2) return MGC_E_INVALID;
+  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
+  int rc = ready(mesh, gas);
+  if (rc) return rc;
+  const DGArgs<R> a =
+      make_args<R>(mesh, q, t_op, nullptr, nullptr, rhs, bext, flux_kind, 0, status);
+  return dispatch(1, mesh, gas, a, (cudaStream_t)stream);
+}
+
+template <class R>
+int ns_grad_impl(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const R* q, const R* t_op,
+                 const R* bext, R* grad, int32_t* status, void* stream) {
+  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !grad || !status) return MGC_E_INVALID;
+  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
+  int rc = ready(mesh, gas);
+  if (rc) return rc;
+  const DGArgs<R> a = make_args<R>(mesh, q, t_op, nullptr, nullptr, grad, bext, 0, 0, status);
+  return dispatch(0, mesh, gas, a, (cudaStream_t)stream);
+}
+
+template <class R>
+int ns_rhs_impl(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const R* q, const R* t_op,
+                const R* t_src, const R* grad, const R* bext, int flux_kind, int add_sources,
+                R* rhs, int32_t* status, void* stream) {
+  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !grad || !rhs || !status) return MGC_E_INVALID;
+  if (flux_kind < 0 || flux_kind > 2) return MGC_E_INVALID;
+  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
+  if (add_sources && (gas->eos_kind != MGC_EOS_MIXTURE || !t_src)) return MGC_E_INVALID;
+  int rc = ready(mesh, gas);
+  if (rc) return rc;
+  const DGArgs<R> a =
+      make_args<R>(mesh, q, t_op, t_src, grad, rhs, bext, flux_kind, add_sources, status);
+  return dispatch(2, mesh, gas, a, (cudaStream_t)stream);
 }
 
 }  // namespace
@@ -134,6 +198,10 @@ int mgc_upload_reference_operators(int dim, int order, const double* weak_host,
   if (rc) return rc;
   rc = tu3_upload_refops(dim, order, p64.data(), p32.data(), fn.data());
   if (rc) return rc;
+  rc = tu2f_upload_refops(dim, order, p64.data(), p32.data(), fn.data());
+  if (rc) return rc;
+  rc = tu3f_upload_refops(dim, order, p64.data(), p32.data(), fn.data());
+  if (rc) return rc;
   rc = upload_refops_local(dim, order, p64.data(), p32.data(), fn.data());
   if (rc) return rc;
   const int dev = current_device();
@@ -151,6 +219,10 @@ int mgc_set_mechanism(const mgc_mechanism_t* mech_host) {
   int rc = tu2_upload_mechanism(&m);
   if (rc) return rc;
   rc = tu3_upload_mechanism(&m);
+  if (rc) return rc;
+  rc = tu2f_upload_mechanism(&m);
+  if (rc) return rc;
+  rc = tu3f_upload_mechanism(&m);
   if (rc) return rc;
   rc = upload_mechanism_local(&m);
   if (rc) return rc;
@@ -178,40 +250,76 @@ int mgc_mixture_temperature(int dim, const mgc_gas_t* gas, int64_t nnodes, const
 int mgc_euler_rhs(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
                   const double* t_op, const double* bext, int flux_kind, double* rhs,
                   int32_t* status, void* stream) {
-  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !rhs || !status) return MGC_E_INVALID;
-  if (flux_kind < 0 || flux_kind > 2) return MGC_E_INVALID;
-  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
-  int rc = ready(mesh, gas);
-  if (rc) return rc;
-  const DGArgs<double> a =
-      make_args(mesh, q, t_op, nullptr, nullptr, rhs, bext, flux_kind, 0, status);
-  return dispatch(1, mesh, gas, a, (cudaStream_t)stream);
+  return euler_rhs_impl<double>(mesh, gas, q, t_op, bext, flux_kind, rhs, status, stream);
+}
+
+int mgc_euler_rhs_f32(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
+                      const float* t_op, const float* bext, int flux_kind, float* rhs,
+                      int32_t* status, void* stream) {
+  return euler_rhs_impl<float>(mesh, gas, q, t_op, bext, flux_kind, rhs, status, stream);
 }
 
 int mgc_ns_grad(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
                 const double* t_op, const double* bext, double* grad, int32_t* status,
                 void* stream) {
-  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !grad || !status) return MGC_E_INVALID;
-  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
-  int rc = ready(mesh, gas);
-  if (rc) return rc;
-  const DGArgs<double> a = make_args(mesh, q, t_op, nullptr, nullptr, grad, bext, 0, 0, status);
-  return dispatch(0, mesh, gas, a, (cudaStream_t)stream);
+  return ns_grad_impl<double>(mesh, gas, q, t_op, bext, grad, status, stream);
+}
+
+int mgc_ns_grad_f32(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
+                    const float* t_op, const float* bext, float* grad, int32_t* status,
+                    void* stream) {
+  return ns_grad_impl<float>(mesh, gas, q, t_op, bext, grad, status, stream);
 }
 
 int mgc_ns_rhs(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
                const double* t_op, const double* t_src, const double* grad,
                const double* bext, int flux_kind, int add_sources, double* rhs,
                int32_t* status, void* stream) {
-  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !grad || !rhs || !status) return MGC_E_INVALID;
-  if (flux_kind < 0 || flux_kind > 2) return MGC_E_INVALID;
-  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
-  if (add_sources && (gas->eos_kind != MGC_EOS_MIXTURE || !t_src)) return MGC_E_INVALID;
-  int rc = ready(mesh, gas);
-  if (rc) return rc;
-  const DGArgs<double> a =
-      make_args(mesh, q, t_op, t_src, grad, rhs, bext, flux_kind, add_sources, status);
-  return dispatch(2, mesh, gas, a, (cudaStream_t)stream);
+  return ns_rhs_impl<double>(mesh, gas, q, t_op, t_src, grad, bext, flux_kind, add_sources,
+                             rhs, status, stream);
+}
+
+int mgc_ns_rhs_f32(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
+                   const float* t_op, const float* t_src, const float* grad,
+                   const float* bext, int flux_kind, int add_sources, float* rhs,
+                   int32_t* status, void* stream) {
+  return ns_rhs_impl<float>(mesh, gas, q, t_op, t_src, grad, bext, flux_kind, add_sources, rhs,
+                            status, stream);
+}
+
+int mgc_mixture_temperature_f32(int dim, const mgc_gas_t* gas, int64_t nnodes, const float* q,
+                                const float* t_seed, const float* t_guess, float* t_out,
+                                int32_t* iters, int maxit, float rtol, int32_t* status,
+                                void* stream) {
+  if (!gas_ok(gas) || gas->eos_kind != MGC_EOS_MIXTURE || nnodes < 0 || !q || !t_seed ||
+      !t_out || !status || maxit < 1 || maxit > 100 || !(rtol > 0.f))
+    return MGC_E_INVALID;
+  if (nnodes == 0) return MGC_OK;
+  const int dev = current_device();
+  if (dev < 0) return MGC_E_CUDA;
+  if (!g_mech_ready[dev]) return MGC_E_NOT_READY;
+  const GasParams p = to_params(gas);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dim == 2)
+    return tu2f_mixture_state(gas->nspecies, nnodes, q, t_seed, t_guess, t_out, iters, maxit,
+                              rtol, status, p, s);
+  if (dim == 3)
+    return tu3f_mixture_state(gas->nspecies, nnodes, q, t_seed, t_guess, t_out, iters, maxit,
+                              rtol, status, p, s);
+  return MGC_E_UNSUPPORTED;
+}
+
+int mgc_rk4_stage_mixed(int64_t n, const double* q0, const float* k, double* sum,
+                        double* q_out, float* q_out_lo, int stage, double dt, void* stream) {
+  if (n < 0 || !q0 || !k || !sum || !q_out || !q_out_lo || stage < 0 || stage > 3)
+    return MGC_E_INVALID;
+  if (n == 0) return MGC_OK;
+  const int nt = 256;
+  int64_t nb = (n + nt - 1) / nt;
+  if (nb > 148 * 32) nb = 148 * 32;
+  k_rk4_stage_mixed<<<(unsigned)nb, nt, 0, (cudaStream_t)stream>>>(n, q0, k, sum, q_out,
+                                                                   q_out_lo, stage, dt);
+  return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
 }
 
 int mgc_rk4_stage(int64_t n, const double* q0, const double* k, double* sum, double* q_out,

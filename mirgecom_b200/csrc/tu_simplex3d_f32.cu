@@ -1,0 +1,30 @@
+// Kernel instantiations for 3-D simplices, mixed-precision path (float32
+// storage and pointwise math, tf32 x3 tensor-core contractions).
+#include "dg_dispatch.cuh"
+
+namespace mgc {
+
+int tu3f_upload_refops(int dim, int order, const double* p64, const float* p32, const int* fn) {
+  return upload_refops_local(dim, order, p64, p32, fn);
+}
+
+int tu3f_upload_mechanism(const Mechanism* m) { return upload_mechanism_local(m); }
+
+int tu3f_dispatch(int op, int order, int ns, bool mix, const DGArgs<float>& a,
+                     const GasParams& g, cudaStream_t s) {
+  switch (order) {
+    case 1: return dispatch_order<float, 3, 1>(op, ns, mix, a, g, s);
+    case 2: return dispatch_order<float, 3, 2>(op, ns, mix, a, g, s);
+    case 3: return dispatch_order<float, 3, 3>(op, ns, mix, a, g, s);
+    default: return MGC_E_UNSUPPORTED;
+  }
+}
+
+int tu3f_mixture_state(int ns, int64_t nnodes, const float* q, const float* tseed,
+                          const float* tguess, float* tout, int32_t* iters, int maxit,
+                          float rtol, int32_t* status, const GasParams& g, cudaStream_t s) {
+  return mixture_state_mixed_dim<3>(ns, nnodes, q, tseed, tguess, tout, iters, maxit, rtol,
+                                       status, g, s);
+}
+
+}  // namespace mgc

@@ -87,7 +87,7 @@ class PyrometheusMixture(MixtureEOS):
     """
 
     def __init__(self, pyrometheus_mech: Mechanism, temperature_guess=300.0,
-                 temperature_niter=5, zero_level=0.0):
+                 temperature_niter=5, zero_level=0.0, learned_guess=None):
         if pyrometheus_mech.nspecies > _lib.MAX_SPECIES \
                 or pyrometheus_mech.nreactions > _lib.MAX_REACTIONS:
             raise ValueError("mechanism too large for the device tables")
@@ -95,6 +95,12 @@ class PyrometheusMixture(MixtureEOS):
         self._tguess = float(temperature_guess)
         self._niter = int(temperature_niter)
         self._zero_level = float(zero_level)
+        # optional learned Newton initial guess (mixed form only), e.g. a
+        # mirgecom_b200.learned_guess.TemperatureMLP
+        self.learned_guess = learned_guess
+
+    def learned_temperature_guess(self, cv):
+        return self.learned_guess.predict(cv)
 
     @property
     def mechanism(self):

@@ -114,6 +114,13 @@ def make_fluid_state(cv: ConservedVars, gas_model: GasModel, temperature_seed=No
                                           "*temperature_seed*.")
     from mirgecom_b200 import runtime
     tseed = eos.get_temperature_seed(cv.mass, temperature_seed)
+    if cv.q.dtype == torch.float32:
+        # mixed form: learned guess (if the EOS carries one), float32 Newton
+        # with adaptive stop, float64 residual check, plain-guess fallback
+        guess = eos.learned_temperature_guess(cv) if eos.learned_guess is not None else None
+        t = runtime.mixture_temperature_mixed(cv, gas_model, tseed, guess,
+                                              iters=kwargs.get("newton_iterations"))
+        return FluidState(cv, gas_model, temperature=t, operator_temperature=t)
     t1, t2 = runtime.mixture_temperature(cv, gas_model, tseed)
     return FluidState(cv, gas_model, temperature=t1, operator_temperature=t2)
 

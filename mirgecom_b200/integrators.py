@@ -37,6 +37,31 @@ def rk4_step(state, t, dt, rhs):
     return ConservedVars(out, state.dim)
 
 
+def rk4_step_mixed(state, t, dt, rhs, state_lo=None):
+    """RK4 of the mixed-precision form.
+
+    *state* is the float64 ConservedVars; *rhs(t, cv32)* takes and returns
+    float32 ConservedVars.  Stage states and the stage sum are accumulated in
+    float64 (the only float64 arithmetic of the form besides the Newton
+    residual check); each stage kernel also emits the float32 copy the next
+    right-hand side reads.  Returns (new float64 state, its float32 copy).
+    """
+    q0 = state.q.contiguous()
+    q32 = state_lo.q if state_lo is not None else q0.to(torch.float32)
+    acc = torch.empty_like(q0)
+    qs = torch.empty_like(q0)
+    qs32 = torch.empty_like(q32)
+    tt = [t + dt / 2, t + dt / 2, t + dt]
+    k = rhs(t, ConservedVars(q32, state.dim))
+    for stage in range(3):
+        runtime.rk4_stage(q0, k.q.contiguous(), acc, qs, stage, dt, qout_lo=qs32)
+        k = rhs(tt[stage], ConservedVars(qs32, state.dim))
+    out = torch.empty_like(q0)
+    out32 = torch.empty_like(q32)
+    runtime.rk4_stage(q0, k.q.contiguous(), acc, out, 3, dt, qout_lo=out32)
+    return ConservedVars(out, state.dim), ConservedVars(out32, state.dim)
+
+
 def advance_state(rhs, timestepper, state, t_final, t=0.0, dt=None, istep=0,
                   pre_step_callback=None, post_step_callback=None, max_steps=None):
     """Thin counterpart of mirgecom/steppers.py:350-449 (fixed dt)."""

@@ -27,6 +27,7 @@ Every operator is returned in the form the DG right-hand side consumes
 
 from __future__ import annotations
 
+import functools
 import itertools
 import math
 from dataclasses import dataclass, field
@@ -327,16 +328,142 @@ def cube_quadrature(dim, nq):
 # }}}
 
 
+# {{{ extended-precision nodal operators
+
+_MP_DPS = 40
+
+
+def _mp_gauss_legendre(n):
+    """n-point Gauss-Legendre rule on [-1, 1] in mpmath precision."""
+    import mpmath as mp
+    xs, ws = [], []
+    for i in range(1, n + 1):
+        x = mp.cos(mp.pi * (i - mp.mpf(1) / 4) / (n + mp.mpf(1) / 2))
+        for _ in range(100):
+            p0, p1 = mp.mpf(1), x
+            for k in range(2, n + 1):
+                p0, p1 = p1, ((2 * k - 1) * x * p1 - (k - 1) * p0) / k
+            dp = n * (x * p1 - p0) / (x * x - 1)
+            dx = p1 / dp
+            x -= dx
+            if abs(dx) < mp.mpf(10) ** (-_MP_DPS + 5):
+                break
+        xs.append(x)
+        ws.append(2 / ((1 - x * x) * dp * dp))
+    return xs, ws
+
+
+def _mp_quadrature(kind, dim, nq):
+    """Gauss rule on the reference simplex (collapsed) or hypercube, mpmath."""
+    import itertools as it
+
+    import mpmath as mp
+    xg, wg = _mp_gauss_legendre(nq)
+    pts, wts = [], []
+    for idx in it.product(range(nq), repeat=dim):
+        c = [xg[i] for i in idx]
+        w = mp.mpf(1)
+        for i in idx:
+            w *= wg[i]
+        if kind == "hypercube" or dim == 1:
+            pts.append(c)
+            wts.append(w)
+        elif dim == 2:
+            a, b = c
+            pts.append([(1 + a) * (1 - b) / 2 - 1, b])
+            wts.append(w * (1 - b) / 2)
+        else:
+            a, b, cc = c
+            t = cc
+            s_ = (1 + b) * (1 - cc) / 2 - 1
+            r = (1 + a) * (-s_ - t) / 2 - 1
+            pts.append([r, s_, t])
+            wts.append(w * (1 - b) / 2 * ((1 - cc) / 2) ** 2)
+    return pts, wts
+
+
+def _mp_basis(point, exponents, order):
+    """Legendre-product basis values and gradients at one point (mpmath)."""
+    import mpmath as mp
+    dim = len(point)
+    pv, dpv = [], []
+    for d in range(dim):
+        x = point[d]
+        p = [mp.mpf(1), x]
+        dp = [mp.mpf(0), mp.mpf(1)]
+        for k in range(1, order):
+            p.append(((2 * k + 1) * x * p[k] - k * p[k - 1]) / (k + 1))
+            dp.append(dp[k - 1] + (2 * k + 1) * p[k])
+        pv.append(p)
+        dpv.append(dp)
+    vals, grads = [], [[] for _ in range(dim)]
+    for e in exponents:
+        v = mp.mpf(1)
+        for d in range(dim):
+            v *= pv[d][e[d]]
+        vals.append(v)
+        for r in range(dim):
+            g = mp.mpf(1)
+            for d in range(dim):
+                g *= dpv[d][e[d]] if d == r else pv[d][e[d]]
+            grads[r].append(g)
+    return vals, grads
+
+
+def _nodal_operators_mp(nodes, exponents, kind, nq):
+    """Vandermonde, exact mass matrix and derivative matrices, computed in
+    mpmath (40 digits) and rounded once to float64; also returns the mpmath
+    mass and derivative matrices for further exact products."""
+    import mpmath as mp
+    mp.mp.dps = _MP_DPS
+    dim, npts = nodes.shape
+    order = max(max(e) for e in exponents)
+    nb = len(exponents)
+    vdm = mp.matrix(npts, nb)
+    gr = [mp.matrix(npts, nb) for _ in range(dim)]
+    for i in range(npts):
+        vals, grads = _mp_basis([mp.mpf(float(nodes[d, i])) for d in range(dim)],
+                                exponents, order)
+        for j in range(nb):
+            vdm[i, j] = vals[j]
+            for r in range(dim):
+                gr[r][i, j] = grads[r][j]
+    vinv = mp.inverse(vdm)
+    qp, qw = _mp_quadrature(kind, dim, nq)
+    # mass = sum_q w_q l_i(x_q) l_j(x_q),  l = interpolants
+    lq = mp.matrix(len(qp), npts)
+    for q, pt in enumerate(qp):
+        vals, _ = _mp_basis(pt, exponents, order)
+        row = mp.matrix([vals])
+        lrow = row * vinv
+        for j in range(npts):
+            lq[q, j] = lrow[0, j]
+    mass = mp.matrix(npts, npts)
+    for q in range(len(qp)):
+        for i in range(npts):
+            wi = qw[q] * lq[q, i]
+            for j in range(npts):
+                mass[i, j] += wi * lq[q, j]
+    diff = [gr[r] * vinv for r in range(dim)]
+    return vdm, mass, diff
+
+
+def _mp_to_np(m):
+    return np.array([[float(m[i, j]) for j in range(m.cols)] for i in range(m.rows)])
+
+
 def _nodal_operators(nodes, exponents, quad):
-    """Interpolation matrices from the modal basis: mass, derivative, W_r."""
+    """float64 interface (kept for the oracle-independent consistency check)."""
     vdm, grads = legendre_basis(nodes, exponents)
     vinv = np.linalg.inv(vdm)
     qx, qw = quad
     vq, _ = legendre_basis(qx, exponents)
-    interp_q = vq @ vinv                              # nodal -> quadrature
-    mass = interp_q.T @ (qw[:, None] * interp_q)      # exact mass matrix
-    diff = np.stack([g @ vinv for g in grads])        # D_r[a, b] = d_r l_b(x_a)
+    interp_q = vq @ vinv
+    mass = interp_q.T @ (qw[:, None] * interp_q)
+    diff = np.stack([g @ vinv for g in grads])
     return vdm, mass, diff
+
+# }}}
 
 
 @dataclass
@@ -407,9 +534,14 @@ def make_simplex_element(dim, order):
     nodes = simplex_nodes(dim, order)
     verts = _simplex_vertices(dim)
     exps = total_degree_exponents(dim, order)
-    vdm, mass, diff = _nodal_operators(nodes, exps, simplex_quadrature(dim, order + 3))
-    mass_inv = np.linalg.inv(mass)
-    weak = np.stack([mass_inv @ d.T @ mass for d in diff])
+    import mpmath as mp
+    vdm_mp, mass_mp, diff_mp = _nodal_operators_mp(nodes, exps, "simplex", order + 3)
+    mass_inv_mp = mp.inverse(mass_mp)
+    vdm = _mp_to_np(vdm_mp)
+    mass = _mp_to_np(mass_mp)
+    mass_inv = _mp_to_np(mass_inv_mp)
+    diff = np.stack([_mp_to_np(d) for d in diff_mp])
+    weak = np.stack([_mp_to_np(mass_inv_mp * d.T * mass_mp) for d in diff_mp])
     faces = _SIMPLEX_FACES[dim]
 
     # face nodes ordered like the (dim-1) reference node set
@@ -435,20 +567,24 @@ def make_simplex_element(dim, order):
 
     # face mass matrix in the face's own reference parametrisation
     if dim == 1:
-        face_mass = np.ones((1, 1))
+        face_mass_mp = mp.matrix([[1]])
         param_area = 1.0
     else:
         fexps = total_degree_exponents(dim - 1, order)
-        _, face_mass, _ = _nodal_operators(
-            fnodes_ref, fexps, simplex_quadrature(dim - 1, order + 3))
-        param_area = 2.0 if dim == 3 else 2.0
+        _, face_mass_mp, _ = _nodal_operators_mp(fnodes_ref, fexps, "simplex", order + 3)
+        param_area = 2.0
+    face_mass = _mp_to_np(face_mass_mp)
 
     npn = nodes.shape[1]
     lift = np.zeros((npn, len(faces) * nfp))
     for f in range(len(faces)):
-        emat = np.zeros((npn, nfp))
-        emat[face_nodes[f], :] = face_mass
-        lift[:, f * nfp:(f + 1) * nfp] = mass_inv @ emat
+        # M^-1 E_f with E_f the face mass placed on the face's volume nodes
+        for i in range(npn):
+            for m in range(nfp):
+                acc = mp.mpf(0)
+                for mm in range(nfp):
+                    acc += mass_inv_mp[i, int(face_nodes[f, mm])] * face_mass_mp[mm, m]
+                lift[i, f * nfp + m] = float(acc)
 
     # reference outward normals and face measures
     centroid = verts.mean(axis=0)
@@ -488,21 +624,44 @@ def _hypercube_vertices(dim):
 
 
 def make_hypercube_element(dim, order):
-    """Tensor-product GLL element; node index = i0 + (p+1) i1 + (p+1)^2 i2."""
+    """Tensor-product GLL element; node index = i0 + (p+1) i1 + (p+1)^2 i2.
+
+    The operators are Kronecker products of 1-D operators computed in
+    mpmath precision (exact mass matrix on the GLL nodes)."""
+    import mpmath as mp
     x1 = jacobi_gl(0, 0, order)
     n1 = order + 1
     grids = np.meshgrid(*([x1] * dim), indexing="ij")
     # axis 0 fastest
     nodes = np.stack([g.transpose(tuple(range(dim))[::-1]).ravel() for g in grids])
-    exps = tensor_exponents(dim, order)
-    vdm, mass, diff = _nodal_operators(nodes, exps, cube_quadrature(dim, order + 2))
-    mass_inv = np.linalg.inv(mass)
-    weak = np.stack([mass_inv @ d.T @ mass for d in diff])
-    # 1-D operators for sum factorisation
-    _, mass1, diff1 = _nodal_operators(x1[None, :], [(i,) for i in range(n1)],
-                                       cube_quadrature(1, order + 2))
-    mass1_inv = np.linalg.inv(mass1)
-    weak1 = mass1_inv @ diff1[0].T @ mass1
+    v1_mp, mass1_mp, diff1_mp = _nodal_operators_mp(
+        x1[None, :], [(i,) for i in range(n1)], "hypercube", order + 2)
+    mass1_inv_mp = mp.inverse(mass1_mp)
+    mass1 = _mp_to_np(mass1_mp)
+    mass1_inv = _mp_to_np(mass1_inv_mp)
+    diff1 = _mp_to_np(diff1_mp[0])
+    weak1 = _mp_to_np(mass1_inv_mp * diff1_mp[0].T * mass1_mp)
+    eye = np.eye(n1)
+
+    def kron_axis(op, axis):
+        # operator acting along `axis` (0 = fastest index)
+        mats = [op if a == axis else eye for a in range(dim)][::-1]
+        out = mats[0]
+        for mmat in mats[1:]:
+            out = np.kron(out, mmat)
+        return out
+
+    def kron_all(op):
+        out = op
+        for _ in range(dim - 1):
+            out = np.kron(out, op)
+        return out
+
+    mass = kron_all(mass1)
+    mass_inv = kron_all(mass1_inv)
+    diff = np.stack([kron_axis(diff1, r) for r in range(dim)])
+    weak = np.stack([kron_axis(weak1, r) for r in range(dim)])
+    vdm = kron_all(_mp_to_np(v1_mp))
 
     # faces: (axis, side) -> f = 2*axis + side
     faces = []
@@ -520,20 +679,22 @@ def make_hypercube_element(dim, order):
         face_mass = np.ones((1, 1))
         param_area = 1.0
     else:
-        other = [a for a in range(dim)]
-        fx = jacobi_gl(0, 0, order)
-        fgr = np.meshgrid(*([fx] * (dim - 1)), indexing="ij")
-        fnodes = np.stack([g.transpose(tuple(range(dim - 1))[::-1]).ravel() for g in fgr])
-        _, face_mass, _ = _nodal_operators(fnodes, tensor_exponents(dim - 1, order),
-                                           cube_quadrature(dim - 1, order + 2))
+        face_mass = mass1 if dim == 2 else np.kron(mass1, mass1)
         param_area = 2.0 ** (dim - 1)
-        del other
     npn = nodes.shape[1]
     lift = np.zeros((npn, len(faces) * nfp))
     for f in range(len(faces)):
-        emat = np.zeros((npn, nfp))
-        emat[face_nodes[f], :] = face_mass
-        lift[:, f * nfp:(f + 1) * nfp] = mass_inv @ emat
+        axis, side = divmod(f, 2)
+        col = 0 if side == 0 else n1 - 1
+        # M^-1 E_f = (M1^-1 e_side along `axis`) x identity on the face axes
+        for m in range(nfp):
+            fnode = face_nodes[f, m]
+            rest = [(fnode // n1 ** a) % n1 for a in range(dim)]
+            for i1 in range(n1):
+                idx = list(rest)
+                idx[axis] = i1
+                vol = sum(idx[a] * n1 ** a for a in range(dim))
+                lift[vol, f * nfp + m] = mass1_inv[i1, col]
     normals = np.zeros((len(faces), dim))
     for axis in range(dim):
         normals[2 * axis, axis] = -1.0
@@ -554,10 +715,12 @@ def make_hypercube_element(dim, order):
         face_mass=face_mass, face_param_area=param_area,
         ref_face_normals=normals, ref_face_areas=areas, ref_volume=2.0 ** dim,
         extra={"vandermonde": vdm, "nodes1d": x1, "mass1d": mass1,
-               "diff1d": diff1[0], "weak1d": weak1, "mass1d_inv": mass1_inv})
+               "diff1d": diff1, "weak1d": weak1, "mass1d_inv": mass1_inv})
 
 
+@functools.lru_cache(maxsize=None)
 def make_reference_element(kind, dim, order):
+    """Cached: the operators are pure functions of (kind, dim, order)."""
     if kind == "simplex":
         return make_simplex_element(dim, order)
     if kind == "hypercube":

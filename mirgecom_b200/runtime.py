@@ -59,6 +59,7 @@ class DeviceDiscretization:
         c = dcoll.connectivity
         g = dcoll.geometry
         self.rx = torch.from_numpy(np.ascontiguousarray(g.rx)).to(device)
+        self.rx32 = self.rx.to(torch.float32)
         self.conn = torch.from_numpy(np.ascontiguousarray(c.conn, dtype=np.int32)).to(device)
         self.perm = torch.from_numpy(np.ascontiguousarray(c.perm, dtype=np.uint8)).to(device)
         nbf = len(c.bface_elem)
@@ -79,6 +80,7 @@ class DeviceDiscretization:
         self.mesh.conn = self.conn.data_ptr()
         self.mesh.perm = self.perm.data_ptr()
         self.mesh.bkind = None
+        self.mesh.rx32 = self.rx32.data_ptr()
 
     def workspace(self, name, shape, dtype=torch.float64):
         t = self._work.get(name)
@@ -116,6 +118,32 @@ def _gas_struct(gas_model, nspecies, device):
     if gas_model.eos.is_mixture:
         ensure_mechanism(gas_model.eos, device)
     return gas_model.to_struct(nspecies)
+
+
+MIXED_NEWTON_MAXIT = 12
+MIXED_NEWTON_RTOL = 1e-6
+
+
+def mixture_temperature_mixed(cv, gas_model, tseed, tguess=None, iters=None, status=None):
+    """Mixed-form temperature: float32 Newton from *tguess* (else *tseed*),
+    float64 residual check, plain-guess fallback.  Returns T (float32)."""
+    q = cv.q
+    _lib.require_cuda(q)
+    lib = _lib.load()
+    gs = _gas_struct(gas_model, cv.nspecies, q.device)
+    n = q[0].numel()
+    tout = torch.empty_like(q[0])
+    tseed = tseed.to(dtype=torch.float32).contiguous()
+    if tguess is not None:
+        tguess = tguess.to(dtype=torch.float32).contiguous()
+    if status is None:
+        status = torch.zeros(1, dtype=torch.int32, device=q.device)
+    with torch.cuda.device(q.device):
+        _lib.check(lib.mgc_mixture_temperature_f32(
+            cv.dim, C.byref(gs), n, _lib.ptr(q), _lib.ptr(tseed), _lib.ptr(tguess),
+            _lib.ptr(tout), _lib.ptr(iters), MIXED_NEWTON_MAXIT, MIXED_NEWTON_RTOL,
+            _lib.ptr(status), _lib.stream_handle()), "mgc_mixture_temperature_f32")
+    return tout
 
 
 def mixture_temperature(cv, gas_model, tseed):
@@ -169,6 +197,9 @@ def boundary_exterior(dd, state, gas_model, boundaries, time):
 def _operator_temperature(state):
     if not state.is_mixture:
         return None
+    if state.cv.q.dtype == torch.float32:
+        # the mixed form carries one temperature for the state and its operator
+        return state.temperature.contiguous()
     if state.operator_temperature is None:
         # the operator states re-solve from the state temperature
         _, t2 = mixture_temperature(state.cv, state.gas_model, state.temperature)
@@ -188,8 +219,9 @@ def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
     bext = boundary_exterior(dd, state, gas_model, boundaries, time)
     t_op = _operator_temperature(state)
     rhs = torch.empty_like(q)
+    fn = lib.mgc_euler_rhs_f32 if q.dtype == torch.float32 else lib.mgc_euler_rhs
     with torch.cuda.device(q.device):
-        _lib.check(lib.mgc_euler_rhs(
+        _lib.check(fn(
             C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(bext),
             flux_kind, _lib.ptr(rhs), _lib.ptr(dd.status), _lib.stream_handle()),
             "mgc_euler_rhs")
@@ -213,19 +245,24 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
     t_op = _operator_temperature(state)
     grad = grad_out if grad_out is not None else dd.workspace(
         "grad", (nc + 1, dcoll.dim) + tuple(q.shape[1:]), q.dtype)
+    if source_temperature is not None:
+        source_temperature = source_temperature.to(q.dtype)
     rhs = torch.empty_like(q)
     stream = _lib.stream_handle()
     add_src = source_temperature is not None
     t_src = source_temperature.contiguous() if add_src else None
+    f32 = q.dtype == torch.float32
+    fgrad = lib.mgc_ns_grad_f32 if f32 else lib.mgc_ns_grad
+    frhs = lib.mgc_ns_rhs_f32 if f32 else lib.mgc_ns_rhs
     with torch.cuda.device(q.device):
         if events:
             events[0].record()
-        _lib.check(lib.mgc_ns_grad(
+        _lib.check(fgrad(
             C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(bext),
             _lib.ptr(grad), _lib.ptr(dd.status), stream), "mgc_ns_grad")
         if events:
             events[1].record()
-        _lib.check(lib.mgc_ns_rhs(
+        _lib.check(frhs(
             C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(t_src),
             _lib.ptr(grad), _lib.ptr(bext), flux_kind, int(add_src), _lib.ptr(rhs),
             _lib.ptr(dd.status), stream), "mgc_ns_rhs")
@@ -247,6 +284,11 @@ def read_status(dcoll, device=None, reset=True):
 def rk4_stage(q0, k, acc, qout, stage, dt, qout_lo=None):
     lib = _lib.load()
     n = q0.numel()
+    if k.dtype == torch.float32:
+        _lib.check(lib.mgc_rk4_stage_mixed(
+            n, _lib.ptr(q0), _lib.ptr(k), _lib.ptr(acc), _lib.ptr(qout), _lib.ptr(qout_lo),
+            stage, float(dt), _lib.stream_handle()), "mgc_rk4_stage_mixed")
+        return
     _lib.check(lib.mgc_rk4_stage(n, _lib.ptr(q0), _lib.ptr(k), _lib.ptr(acc), _lib.ptr(qout),
                                  _lib.ptr(qout_lo), stage, float(dt), _lib.stream_handle()),
                "mgc_rk4_stage")
@@ -266,8 +308,9 @@ def ns_gradients(dcoll, state, gas_model, boundaries, time):
     bext = boundary_exterior(dd, state, gas_model, boundaries, time)
     t_op = _operator_temperature(state)
     grad = dd.workspace("grad", (nc + 1, dcoll.dim) + tuple(q.shape[1:]), q.dtype)
+    fgrad = lib.mgc_ns_grad_f32 if q.dtype == torch.float32 else lib.mgc_ns_grad
     with torch.cuda.device(q.device):
-        _lib.check(lib.mgc_ns_grad(
+        _lib.check(fgrad(
             C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(bext),
             _lib.ptr(grad), _lib.ptr(dd.status), _lib.stream_handle()), "mgc_ns_grad")
     return grad

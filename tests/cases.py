@@ -82,3 +82,26 @@ def perturbed_state_np(x, dim, nspecies, seed=0):
     for s in range(nspecies):
         q.append(rho * (0.1 + 0.05 * (s + 1) * (1 + f(5))))
     return np.array(q)
+
+
+def per_field_rel_l2(a, b, floor=None):
+    """Per-field relative L2 errors (same normalisation as field_rel_l2)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    big = max(np.linalg.norm(b[c].ravel()) for c in range(b.shape[0]))
+    out = []
+    for c in range(b.shape[0]):
+        fl = 1e-3 * big if floor is None else floor[c]
+        den = max(np.linalg.norm(b[c].ravel()), fl, 1e-300)
+        out.append(float(np.linalg.norm((a[c] - b[c]).ravel()) / den))
+    return out
+
+
+def flux_scale_floor(q, dim, h, gamma=1.4):
+    """Per-field natural scale of a divergence of the ideal-gas inviscid
+    flux: |F_c| / h (for low-Mach states the RHS is orders of magnitude
+    below its fluxes and roundoff scales with the fluxes)."""
+    from oracle import physics as oph
+    st = oph.make_fluid_state(q, oph.IdealGas(gamma=gamma), None, dim)
+    f = oph.inviscid_flux(st)
+    return [np.linalg.norm(f[c]) / h for c in range(q.shape[0])]
