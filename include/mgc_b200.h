@@ -27,6 +27,7 @@
 #ifndef MGC_B200_H
 #define MGC_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -38,6 +39,7 @@ extern "C" {
 #define MGC_E_UNSUPPORTED (-2)
 #define MGC_E_NOT_READY (-3)
 #define MGC_E_CUDA (-4)
+#define MGC_E_TOO_LARGE (-5)
 
 #define MGC_ST_NAN 1
 #define MGC_ST_BAD_INDEX 2
@@ -189,6 +191,26 @@ int mgc_mixture_temperature_f32(int dim, const mgc_gas_t* gas, int64_t nnodes,
 int mgc_rk4_stage_mixed(int64_t n, const double* q0, const float* k, double* sum,
                         double* q_out, float* q_out_lo, int stage, double dt,
                         void* stream);
+
+/* ---- Navier-Stokes right-hand side without device allocation.
+ * No counterpart in the reference: it exists for callers that cannot
+ * allocate device memory -- a solver that owns all device memory through
+ * its own pool and forbids driver allocations during a run, or a host code
+ * linked without a CUDA allocation layer.  It runs mgc_ns_grad then
+ * mgc_ns_rhs with the gradient buffer taken from a fixed library-owned
+ * device array of mgc_ns_operator_noalloc_capacity() doubles (32 MiB, held
+ * by every GPU that loads the library until exit).  Meshes whose gradient
+ * buffer ((Nc+1)*dim*E*Np doubles) exceeds it return MGC_E_TOO_LARGE.
+ * All calls share that array: calls overlapping on the GPU race and must be
+ * serialised by the caller.  The first call on a device looks up the
+ * array's device address; make it before any stream capture.  Arguments
+ * and results are those of mgc_ns_rhs. ---- */
+size_t mgc_ns_operator_noalloc_capacity(void);
+
+int mgc_ns_operator_noalloc(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
+                            const double* t_op, const double* t_src, const double* bext,
+                            int flux_kind, int add_sources, double* rhs, int32_t* status,
+                            void* stream);
 
 #ifdef __cplusplus
 }

@@ -23,7 +23,8 @@ TR_NONE, TR_SIMPLE, TR_POWERLAW = 0, 1, 2
 FLUX_RUSANOV, FLUX_HLL, FLUX_CENTRAL = 0, 1, 2
 
 ERRORS = {-1: "invalid argument", -2: "unsupported configuration",
-          -3: "reference operators or mechanism not uploaded", -4: "CUDA error"}
+          -3: "reference operators or mechanism not uploaded", -4: "CUDA error",
+          -5: "mesh too large for the fixed no-allocation scratch array"}
 
 ST_NAN, ST_BAD_INDEX, ST_NEWTON_MISS = 1, 2, 4
 
@@ -84,6 +85,9 @@ _SIGNATURES = {
     "mgc_mixture_temperature_f32": (
         [C.c_int, _P, C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_float, _P, _P], C.c_int),
     "mgc_rk4_stage_mixed": ([C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_double, _P], C.c_int),
+    "mgc_ns_operator_noalloc_capacity": ([], C.c_size_t),
+    "mgc_ns_operator_noalloc": (
+        [_P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P], C.c_int),
 }
 
 _lib = None
