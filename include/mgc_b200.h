@@ -175,12 +175,14 @@ int mgc_ns_rhs_f32(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
                    const float* bext, int flux_kind, int add_sources, float* rhs,
                    int32_t* status, void* stream);
 
-/* Mixture temperature, mixed form: float32 Newton with an adaptive stop,
- * started from t_guess (the learned guess; NULL to start from t_seed), a
- * float64 residual check |e - e(T)| / (c_v T) <= rtol, and the plain guess
- * t_seed as fallback when the check fails.  iters (nullable) receives the
- * iteration count per node (+1000 when the fallback ran); nodes failing
- * both set MGC_ST_NEWTON_MISS. */
+/* Mixture temperature, mixed form: float32 Newton started from t_guess (the
+ * learned guess; NULL to start from t_seed) and stopped once the update is
+ * below 1e-5 of T, then a float64 residual check |e - e(T)| / (c_v T) <=
+ * rtol that accepts the result and applies the float64 residual as a last
+ * Newton step (remaining error of order rtol^2); a rejected result is
+ * recomputed from the plain guess t_seed.  iters (nullable) receives the
+ * float32 iteration count per node (+1000 when the fallback ran); nodes
+ * failing both set MGC_ST_NEWTON_MISS. */
 int mgc_mixture_temperature_f32(int dim, const mgc_gas_t* gas, int64_t nnodes,
                                 const float* q, const float* t_seed, const float* t_guess,
                                 float* t_out, int32_t* iters, int maxit, float rtol,
@@ -191,6 +193,44 @@ int mgc_mixture_temperature_f32(int dim, const mgc_gas_t* gas, int64_t nnodes,
 int mgc_rk4_stage_mixed(int64_t n, const double* q0, const float* k, double* sum,
                         double* q_out, float* q_out_lo, int stage, double dt,
                         void* stream);
+
+/* ---- learned initial guess of the mixture temperature (no counterpart in
+ * the reference, whose Newton solve always starts from the seed): an
+ * 8 -> 64 -> 64 -> 1 tanh MLP, bf16 tensor-core matrix products with float32
+ * accumulation.  Inputs: mixture internal energy and the 7 species mass
+ * fractions, normalised by (x - in_shift) * in_scale; output T = out_shift +
+ * out_scale * y.  params is the float32 master vector (mgc_mlp_nparams()
+ * entries: W1 [64][16] with input columns 8..15 zero, b1 [64], W2 [64][64],
+ * b2 [64], w3 [64], b3); the bf16 copies are refreshed by mgc_mlp_refresh
+ * and by every mgc_mlp_adam step. ---- */
+typedef struct {
+  float* params;
+  void* w1_bf16;            /* [64][16] */
+  void* w2_bf16;            /* [64][64] (out, in) */
+  void* w2t_bf16;           /* [64][64] (in, out) */
+  float in_shift[8], in_scale[8];
+  float out_shift, out_scale;
+} mgc_mlp_t;
+
+int mgc_mlp_nparams(void);
+int mgc_mlp_refresh(const mgc_mlp_t* w, void* stream);
+
+/* Guess T for every node of a float32 state q [Nc][n] (nspecies == 7). */
+int mgc_mlp_infer(int dim, int nspecies, int64_t n, const float* q, const mgc_mlp_t* w,
+                  float* t_out, void* stream);
+
+/* Gradient of the mean squared error over n normalised samples x [n][8],
+ * target [n]: grad (mgc_mlp_nparams() floats, overwritten) and loss (one
+ * float, overwritten).  workspace: caller-provided device memory of
+ * mgc_mlp_train_workspace_bytes(n) bytes. */
+size_t mgc_mlp_train_workspace_bytes(int64_t n);
+int mgc_mlp_train_grad(int64_t n, const float* x, const float* target, const mgc_mlp_t* w,
+                       void* workspace, size_t workspace_bytes, float* grad, float* loss,
+                       void* stream);
+
+/* One Adam step on the master vector (m, v: optimiser state, step >= 1). */
+int mgc_mlp_adam(const mgc_mlp_t* w, const float* grad, float* m, float* v, float lr,
+                 float beta1, float beta2, float eps, int step, void* stream);
 
 /* ---- Navier-Stokes right-hand side without device allocation.
  * No counterpart in the reference: it exists for callers that cannot

@@ -67,6 +67,14 @@ class MeshStruct(C.Structure):
     ]
 
 
+class MLPStruct(C.Structure):
+    _fields_ = [
+        ("params", C.c_void_p), ("w1_bf16", C.c_void_p), ("w2_bf16", C.c_void_p),
+        ("w2t_bf16", C.c_void_p), ("in_shift", C.c_float * 8), ("in_scale", C.c_float * 8),
+        ("out_shift", C.c_float), ("out_scale", C.c_float),
+    ]
+
+
 _P = C.c_void_p
 _SIGNATURES = {
     "mgc_version": ([], C.c_int),
@@ -85,6 +93,13 @@ _SIGNATURES = {
     "mgc_mixture_temperature_f32": (
         [C.c_int, _P, C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_float, _P, _P], C.c_int),
     "mgc_rk4_stage_mixed": ([C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_double, _P], C.c_int),
+    "mgc_mlp_nparams": ([], C.c_int),
+    "mgc_mlp_refresh": ([_P, _P], C.c_int),
+    "mgc_mlp_infer": ([C.c_int, C.c_int, C.c_int64, _P, _P, _P, _P], C.c_int),
+    "mgc_mlp_train_workspace_bytes": ([C.c_int64], C.c_size_t),
+    "mgc_mlp_train_grad": ([C.c_int64, _P, _P, _P, _P, C.c_size_t, _P, _P, _P], C.c_int),
+    "mgc_mlp_adam": ([_P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, _P],
+                     C.c_int),
     "mgc_ns_operator_noalloc_capacity": ([], C.c_size_t),
     "mgc_ns_operator_noalloc": (
         [_P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P], C.c_int),

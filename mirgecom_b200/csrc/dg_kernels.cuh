@@ -257,13 +257,16 @@ __global__ void __launch_bounds__(256) k_mixture_state(int64_t nnodes, const R* 
   }
 }
 
-// mixed form: float32 Newton with an adaptive stop from the learned guess
-// (if given) else the seed; the float64 residual check
+// mixed form: float32 Newton from the learned guess (if given) else the
+// seed, stopped once the update falls below 1e-5 of T (float32 cannot
+// resolve e_mix(T) much further once formation enthalpies of ~1e7 J/kg enter
+// e); then the float64 residual check
 //   |e(q) - e_mix(T)| / (c_v(T) T) <= rtol
-// accepts the result, otherwise the plain guess (seed) is iterated instead.
-// iters (optional) receives the float32 iteration count per node, with
-// 1000 added when the fallback ran; ST_NEWTON_MISS flags nodes that fail
-// both.
+// accepts the result and applies that float64 residual as the final Newton
+// step (quadratic convergence: the remaining error is of order rtol^2).  A
+// rejected result is recomputed from the plain guess (seed).  iters
+// (optional) receives the float32 iteration count per node, with 1000
+// added when the fallback ran; ST_NEWTON_MISS flags nodes that fail both.
 template <int DIM, int NS>
 __global__ void __launch_bounds__(256) k_mixture_state_mixed(
     int64_t nnodes, const float* __restrict__ q, const float* __restrict__ tseed,
@@ -300,11 +303,10 @@ __global__ void __launch_bounds__(256) k_mixture_state_mixed(
         const float dt = (e32 - em) / cv;
         t += dt;
         ++used;
-        if (fabsf(dt) <= rtol * 0.25f * fabsf(t)) break;
+        if (fabsf(dt) <= 1e-5f * fabsf(t)) break;
       }
       // float64 residual check; an accepted result takes the float64
-      // residual as one last Newton correction (float32 cannot resolve e(T)
-      // below ~1e-6 relative once formation enthalpies enter e)
+      // residual as its last Newton step
       double em, cv;
       mixture_e_cv<double, NS>(yd, (double)t, em, cv);
       const double corr = (e64 - em) / cv;

@@ -121,7 +121,7 @@ def _gas_struct(gas_model, nspecies, device):
 
 
 MIXED_NEWTON_MAXIT = 12
-MIXED_NEWTON_RTOL = 1e-6
+MIXED_NEWTON_RTOL = 1e-3
 
 
 def mixture_temperature_mixed(cv, gas_model, tseed, tguess=None, iters=None, status=None):
