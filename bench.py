@@ -57,6 +57,10 @@ WORKLOADS = {
         desc="3-D reacting Navier-Stokes, uiuc_7sp, 40^3 hexes x 6 tets (384,000 tets), "
              "order 2 (10 nodes/tet), same fields and models as reacting_p3_tet80",
         n=40, order=2, kind="reacting"),
+    "reacting_p3_tet20": dict(
+        desc="3-D reacting Navier-Stokes, uiuc_7sp, 20^3 hexes x 6 tets (48,000 tets), "
+             "order 3 (20 nodes/tet): the reacting_p3_tet80 physics at a size for profiling",
+        n=20, order=3, kind="reacting"),
     "tgv_p3_tet24": dict(
         desc="3-D viscous Taylor-Green vortex, periodic [-pi,pi]^3, 24^3 hexes x 6 tets "
              "(82,944 tets), order 3 (20 nodes/tet), ideal gas gamma=1.4, Mach 0.1, "
@@ -305,11 +309,48 @@ def _time_form(dcoll, gas, q, tseed, steps, warmup, flush, stream):
     return float(np.sum(step_ms)), kern
 
 
+def _newton_stats(dcoll, gas, q, tseed):
+    """Float32 Newton iterations per node for one temperature solve."""
+    import torch
+
+    from mirgecom_b200.fluid import ConservedVars
+    from mirgecom_b200.gas_model import make_fluid_state
+    it = torch.zeros(q[0].shape, dtype=torch.int32, device=q.device)
+    make_fluid_state(ConservedVars(q, 3), gas, temperature_seed=tseed, newton_iterations=it)
+    fb = it >= 1000
+    base = torch.where(fb, it - 1000, it).float()
+    return {"mean": float(base.mean()), "max": int(base.max()),
+            "fallback_nodes": int(fb.sum())}
+
+
+def _train_guess(dev, seed=0):
+    import torch
+
+    from mirgecom_b200.learned_guess import TemperatureMLP
+    from mirgecom_b200.thermochemistry import UIUC_7SP
+    t0 = time.perf_counter()
+    net = TemperatureMLP(dev, seed=seed)
+    e, y, t = TemperatureMLP.training_pairs(UIUC_7SP, 1 << 20, dev, seed=seed)
+    hist = net.fit(e, y, t, steps=2000, batch=65536, lr=3e-3, seed=seed)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    from mirgecom_b200.fluid import ConservedVars
+    e2, y2, t2 = TemperatureMLP.training_pairs(UIUC_7SP, 1 << 16, dev, seed=seed + 1)
+    q = torch.cat([torch.ones_like(e2)[None], e2[None],
+                   torch.zeros((3, e2.numel()), dtype=torch.float64, device=dev), y2])
+    guess = net.predict(ConservedVars(q.float().contiguous(), 3))
+    rms = float(((guess.double() - t2) ** 2).mean().sqrt())
+    return net, {"samples": 1 << 20, "steps": 2000, "train_s": train_s,
+                 "loss_first": hist[0], "loss_final": hist[-1], "heldout_rms_K": rms}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
 
     from mirgecom_b200 import runtime
+    from mirgecom_b200.eos import PyrometheusMixture
+    from mirgecom_b200.gas_model import GasModel
 
     rank, world, local = _dist_env()
     if world > 1:
@@ -329,30 +370,62 @@ def run_ours(args):
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
+    learned = None
+    gas_learn = None
+    if mixture and not args.profile:
+        net, learned = _train_guess(dev)
+        eos = gas.eos
+        gas_learn = GasModel(eos=PyrometheusMixture(eos.mechanism,
+                                                    temperature_niter=eos.temperature_niter,
+                                                    learned_guess=net),
+                             transport=gas.transport)
+
+    forms = [("plain_fp64", gas, q64, t64), ("mixed_plain_guess", gas, q32, t32)]
+    if mixture and not args.profile:
+        forms.append(("mixed_learned", gas_learn, q32, t32))
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    res = {}
     with ClockSampler(local) as clk:
-        ms64, k64 = _time_form(dcoll, gas, q64, t64, args.steps, args.warmup, flush, stream)
-        ms32, k32 = _time_form(dcoll, gas, q32, t32, args.steps, args.warmup, flush, stream)
+        for name, g, q, t in forms:
+            res[name] = _time_form(dcoll, g, q, t, args.steps, args.warmup, flush, stream)
     if world > 1:
         dist.barrier()
     status = runtime.read_status(dcoll, dev)
+    names = [f[0] for f in forms]
+    tot = [res[n][0] for n in names]
     if world > 1:
-        t = torch.tensor([ms64, ms32], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms64, ms32 = [float(v) for v in t.tolist()]
-    value64 = world * dof * args.steps / (ms64 / 1e3)
-    value32 = world * dof * args.steps / (ms32 / 1e3)
+        tt = torch.tensor(tot, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot = [float(v) for v in tt.tolist()]
+    values = {n: world * dof * args.steps / (ms / 1e3) for n, ms in zip(names, tot)}
+    head = "mixed_learned" if gas_learn is not None else "mixed_plain_guess"
+    hq, ht, hgas = q32, t32, (gas_learn if gas_learn is not None else gas)
+    if args.profile:
+        print(json.dumps({"profile_run": args.workload, "values": values,
+                          "kernels_ms": {n: res[n][1] for n in names}}), flush=True)
+        return
 
-    # end to end through the public API with host buffers (mixed form: the
+    if gas_learn is not None:
+        from mirgecom_b200.initializers import reacting_mixture_state  # noqa: F401
+        cold = torch.full_like(t32, 300.0)
+        learned["newton_warm_seed"] = {
+            "plain_guess": _newton_stats(dcoll, gas, q32, t32),
+            "learned_guess": _newton_stats(dcoll, gas_learn, q32, t32)}
+        learned["newton_cold_start_300K"] = {
+            "plain_guess": _newton_stats(dcoll, gas, q32, cold),
+            "learned_guess": _newton_stats(dcoll, gas_learn, q32, cold)}
+        learned["fp64_plain_iterations"] = "fixed 5 (+5 for the operator states)"
+
+    # end to end through the public API with host buffers (headline form: the
     # float32 state goes in, the float32 right-hand side comes out)
-    q_host = q32.cpu().pin_memory()
+    q_host = hq.cpu().pin_memory()
     out_host = torch.empty_like(q_host).pin_memory()
-    qd = torch.empty_like(q32)
+    qd = torch.empty_like(hq)
     for _ in range(2):
         qd.copy_(q_host, non_blocking=True)
-        out_host.copy_(_rhs_call(dcoll, gas, qd, t32), non_blocking=True)
+        out_host.copy_(_rhs_call(dcoll, hgas, qd, ht), non_blocking=True)
     torch.cuda.synchronize()
     e2e_ms = 0.0
     ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -360,19 +433,21 @@ def run_ours(args):
         flush.fill_(float(i))
         ev[0].record(stream)
         qd.copy_(q_host, non_blocking=True)
-        out_host.copy_(_rhs_call(dcoll, gas, qd, t32), non_blocking=True)
+        out_host.copy_(_rhs_call(dcoll, hgas, qd, ht), non_blocking=True)
         ev[1].record(stream)
         torch.cuda.synchronize()
         e2e_ms += ev[0].elapsed_time(ev[1])
     e2e_value = world * dof * args.steps / (e2e_ms / 1e3)
 
-    # roofline of the dominant kernel of the headline (mixed) form
+    # roofline of the dominant kernel of the headline form
     hbm, peak_kind = _peaks()
     ab = algorithmic_bytes(dcoll, nc, s=4, mixture=mixture)
+    k32 = res[head][1]
     kt = {k: v for k, v in k32.items() if k in ab}
     top = max(kt, key=kt.get)
     achieved = ab[top] / (kt[top] / 1e3) / 1e9
     ab64 = algorithmic_bytes(dcoll, nc, s=8, mixture=mixture)
+    k64 = res["plain_fp64"][1]
     kt64 = {k: v for k, v in k64.items() if k in ab64}
     top64 = max(kt64, key=kt64.get)
     traffic = None
@@ -384,29 +459,34 @@ def run_ours(args):
     if rank != 0:
         return
     cpu = cpu_baseline(args.workload) if world == 1 and not args.no_cpu else None
-    launches_per_step = 3 if mixture else 2
+    launches_per_step = {"plain_fp64": 3 if mixture else 2,
+                         "mixed_plain_guess": 3 if mixture else 2,
+                         "mixed_learned": 4}
     line = {
-        "metric": "DOF-RHS evals/s", "value": value32, "unit": "DOF-RHS/s",
+        "metric": "DOF-RHS evals/s", "value": values[head], "unit": "DOF-RHS/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+tf32x3 (f64 Newton residual, f64 sources)",
+        "ms_per_step": tot[names.index(head)] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+tf32x3 (f64 RK, f64 Newton residual, f64 sources)",
         "data": "synthetic",
         "config": {"workload": args.workload, "desc": w["desc"],
                    "elements": dcoll.nelements, "dof": dof,
-                   "form": "mixed precision, plain-guess Newton",
+                   "form": head.replace("_", " "),
                    "l2": "flushed between timed steps (512 MiB write, untimed)",
                    "parallelism": f"replicas x{world}"},
-        "plain_fp64": {"value": value64, "ms_per_step": ms64 / args.steps, "kernels_ms": k64,
-                       "roofline_frac": ab64[top64] / (kt64[top64] / 1e3) / 1e9 / hbm,
-                       "dominant_kernel": top64},
-        "mixed_over_fp64": value32 / value64,
+        "forms": {n: {"value": values[n], "ms_per_step": ms / args.steps,
+                      "kernels_ms": res[n][1]} for n, ms in zip(names, tot)},
+        "mixed_over_fp64": values[head] / values["plain_fp64"],
         "kernels_ms": k32,
+        "learned_guess": learned,
         "e2e": {"value": e2e_value, "unit": "DOF-RHS/s",
-                "h2d_bytes_per_step": q32.numel() * 4, "d2h_bytes_per_step": q32.numel() * 4},
-        "gpu_launches": 2 * launches_per_step * args.steps,
+                "h2d_bytes_per_step": hq.numel() * 4, "d2h_bytes_per_step": hq.numel() * 4},
+        "gpu_launches": sum(launches_per_step[n] for n in names) * args.steps,
         "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                      "algorithmic_bytes": ab[top], "traffic": traffic},
+        "roofline_plain_fp64": {"kernel": top64,
+                                "frac": ab64[top64] / (kt64[top64] / 1e3) / 1e9 / hbm},
         "device_status": status,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
@@ -424,6 +504,9 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="time the plain and mixed forms only (no network training, "
+                         "end-to-end or CPU legs): the command profiled with ncu")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         run_reference(args)

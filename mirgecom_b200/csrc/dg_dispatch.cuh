@@ -4,13 +4,40 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "dg_kernels.cuh"
 #include "../../include/mgc_b200.h"
 
 namespace mgc {
 
 static_assert(sizeof(GasParams) == sizeof(mgc_gas_t), "gas struct mismatch");
-static_assert(sizeof(Mechanism) == sizeof(mgc_mechanism_t), "mechanism struct mismatch");
+// device mechanism = the C ABI table followed by derived coefficient tables
+inline Mechanism expand_mechanism(const mgc_mechanism_t& m) {
+  Mechanism d;
+  memset(&d, 0, sizeof(d));
+  memcpy(&d, &m, sizeof(m));
+  for (int s = 0; s < MGC_MAX_SPECIES; ++s) {
+    for (int r = 0; r < 2; ++r) {
+      const double* a = r ? m.a_hi[s] : m.a_lo[s];
+      double* h = r ? d.h_hi[s] : d.h_lo[s];
+      double* e = r ? d.s_hi[s] : d.s_lo[s];
+      h[0] = a[0];
+      h[1] = a[1] / 2;
+      h[2] = a[2] / 3;
+      h[3] = a[3] / 4;
+      h[4] = a[4] / 5;
+      h[5] = a[5];
+      e[0] = a[0];
+      e[1] = a[1];
+      e[2] = a[2] / 2;
+      e[3] = a[3] / 3;
+      e[4] = a[4] / 4;
+      e[5] = a[6];
+    }
+  }
+  return d;
+}
 
 inline int upload_refops_local(int dim, int order, const double* packed64, const float* packed32,
                                const int* fnodes) {
@@ -55,6 +82,24 @@ struct Launch {
     return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
   }
   template <bool VISC>
+  static int rhs_split(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
+    const int64_t nn = (int64_t)a.nelem * C::NP;
+    int64_t nb = (nn + 127) / 128;
+    if (nb > 148 * 64) nb = 148 * 64;
+    k_node_flux<R, DIM, ORDER, NS, MIX, VISC><<<(unsigned)nb, 128, 0, s>>>(a, g);
+    if (cudaGetLastError() != cudaSuccess) return MGC_E_CUDA;
+    const size_t smem = C::smem_surface(a.nperm);
+    auto kern = k_surface<R, DIM, ORDER, NS, MIX, VISC>;
+    int rc = prepare_kernel(kern, smem);
+    if (rc) return rc;
+    const int nblk = (a.nelem + C::EPB_SURF - 1) / C::EPB_SURF;
+    kern<<<nblk, C::NT, smem, s>>>(a, g);
+    return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+  }
+  static size_t split_workspace_bytes(int64_t nelem) {
+    return ((size_t)nelem * C::NP * C::FW + (size_t)NS * nelem * C::NP) * sizeof(R) + 256;
+  }
+  template <bool VISC>
   static int rhs(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
     const size_t smem = C::smem_rhs(a.nperm);
     auto kern = k_rhs<R, DIM, ORDER, NS, MIX, VISC>;
@@ -75,7 +120,9 @@ inline int dispatch_order(int op, int ns, bool mix, const DGArgs<R>& a, const Ga
     using L = Launch<R, DIM, ORDER, NSV, MIXV>;                          \
     if (op == 0) return L::grad(a, g, s);                                \
     if (op == 1) return L::template rhs<false>(a, g, s);                 \
-    return L::template rhs<true>(a, g, s);                               \
+    if (op == 2) return L::template rhs<true>(a, g, s);                  \
+    if (op == 3) return L::template rhs_split<false>(a, g, s);           \
+    return L::template rhs_split<true>(a, g, s);                         \
   }
   if constexpr (sizeof(R) == 8) {
     MGC_CASE(0, false)
@@ -88,6 +135,23 @@ inline int dispatch_order(int op, int ns, bool mix, const DGArgs<R>& a, const Ga
   }
 #undef MGC_CASE
   return MGC_E_UNSUPPORTED;
+}
+
+template <class R, int DIM, int ORDER>
+inline size_t split_workspace_order(int ns, bool mix, int64_t nelem) {
+#define MGC_WS(NSV, MIXV) \
+  if (ns == NSV && mix == MIXV) return Launch<R, DIM, ORDER, NSV, MIXV>::split_workspace_bytes(nelem);
+  if constexpr (sizeof(R) == 8) {
+    MGC_WS(0, false)
+    MGC_WS(2, false)
+    MGC_WS(7, false)
+    MGC_WS(7, true)
+  } else {
+    MGC_WS(0, false)
+    MGC_WS(7, true)
+  }
+#undef MGC_WS
+  return 0;
 }
 
 inline bool supported_species(int ns, bool mix) {

@@ -52,6 +52,8 @@ struct DGArgs {
   int32_t* status;
   int32_t add_sources;
   int32_t pad_;
+  R* fbuf;             // split path: per-node flux record [E*NP][FW]
+  R* srcbuf;           // split path: species sources [NS][E][NP]
 };
 
 enum BoundaryKind { BK_DUMMY = 0, BK_PRESCRIBED = 1 };
@@ -121,11 +123,30 @@ struct Cfg {
   static constexpr int KRR = round_up(KR, T::KSTEP);
   static constexpr int KB = T::stride(KRR);
   static constexpr int R_MAT = NAC * MP * KB;
-  static constexpr int R_PER_ELEM = NC * KB + NC * NP + (MIX ? 2 * NP : 0) + NS * NP + GEO;
+  static constexpr int R_PER_ELEM =
+      NC * KB + NC * NP + (MIX ? 2 * NP : 0) + NS * NP + 3 * NP + GEO;
   static constexpr int EPB_R_RAW = (SMEM_BUDGET / RB - R_MAT - 1024 / RB) / R_PER_ELEM;
   static constexpr int EPB_RHS = imax(4, imin(32, EPB_R_RAW >= 8 ? EPB_R_RAW / 8 * 8
                                                                  : EPB_R_RAW / 4 * 4));
   static constexpr int NCOL_R = round_up(NC * EPB_RHS, 8);
+
+  // split right-hand side: per-node flux record = total flux F[c][j] then
+  // p, c, gamma (padded to 16 bytes); the surface kernel holds only the
+  // contraction operands in shared memory
+  static constexpr int FW = round_up(NC * DIM + 3, 4);
+  static constexpr int S_BUDGET = 74 * 1024;
+  // resident blocks: float64 mixture state needs more registers per thread
+  static constexpr int MINB_NODE = (RB == 8 && NS > 2) ? 3 : 4;
+  static constexpr int MINB_SURF = (RB == 8 && NS > 2) ? 1 : 2;
+  static constexpr int S_PER_ELEM = NC * KB + GEO;
+  static constexpr int EPB_S_RAW = (S_BUDGET / RB - R_MAT - 1024 / RB) / S_PER_ELEM;
+  static constexpr int EPB_SURF = imax(4, imin(32, EPB_S_RAW >= 8 ? EPB_S_RAW / 8 * 8
+                                                                  : EPB_S_RAW / 4 * 4));
+  static constexpr int NCOL_S = round_up(NC * EPB_SURF, 8);
+  static size_t smem_surface(int nperm) {
+    return (size_t)(R_MAT + NCOL_S * KB + EPB_SURF * GEO) * RB + NFN * 4 + (size_t)nperm * NFP +
+           64;
+  }
 
   static size_t smem_grad(int nperm) {
     return (size_t)(G_MAT + NCOL_G * (KU + KS) + EPB_GRAD * GEO) * RB + NFN * 4 +
@@ -133,7 +154,7 @@ struct Cfg {
   }
   static size_t smem_rhs(int nperm) {
     return (size_t)(R_MAT + NCOL_R * KB +
-                    EPB_RHS * (NC * NP + (MIX ? 2 * NP : 0) + NS * NP + GEO)) * RB +
+                    EPB_RHS * (NC * NP + (MIX ? 2 * NP : 0) + NS * NP + 3 * NP + GEO)) * RB +
            NFN * 4 + (size_t)nperm * NFP + 64;
   }
 };
@@ -560,7 +581,8 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
   R* q_s = bm + NCOL * KB;                                 // [NC][EPB][NP]
   R* t_s = q_s + NC * EPB * NP;                            // [2][EPB][NP] (MIX)
   R* src_s = t_s + (MIX ? 2 * EPB * NP : 0);               // [NS][EPB][NP] (MIX)
-  R* rx_s = src_s + NS * EPB * NP;                         // [EPB][DIM][DIM]
+  R* pcg_s = src_s + NS * EPB * NP;                        // [3][EPB][NP] p, c, gamma
+  R* rx_s = pcg_s + 3 * EPB * NP;                          // [EPB][DIM][DIM]
   R* nrm_s = rx_s + EPB * DIM * DIM;
   R* fs_s = nrm_s + EPB * NF * DIM;
   int* fn_s = reinterpret_cast<int*>(fs_s + EPB * NF);
@@ -608,6 +630,9 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
     for (int c = 0; c < NC; ++c) qq[c] = q_s[(c * EPB) * NP + idx];
     NodeState<R, DIM, NS> st;
     make_state<R, DIM, NS>(qq, MIX ? t_s[idx] : R(0), g, st);
+    pcg_s[idx] = st.p;
+    pcg_s[EPB * NP + idx] = st.c;
+    pcg_s[2 * EPB * NP + idx] = st.gamma;
     R fl[NC][DIM];
     inviscid_flux<R, DIM, NS>(st, fl);
 #pragma unroll
@@ -641,16 +666,10 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
       }
     if constexpr (MIX && NS > 0) {
       if (sources) {
-        // Arrhenius sources in float64 on both paths: near-equilibrium
-        // forward/reverse cancellation and exp(-Ta/T) would amplify float32
-        // rounding (the mixed form keeps only flux/EOS math in float32)
-        double om[NS], yd[NS];
-        const double rhod = (double)qq[0];
+        R om[NS];
+        production_rates<R, NS>(st.rho, t_s[EPB * NP + idx], st.y, (R)g.zero_level, om);
 #pragma unroll
-        for (int s = 0; s < NS; ++s) yd[s] = (double)qq[2 + DIM + s] / rhod;
-        production_rates<double, NS>(rhod, (double)t_s[EPB * NP + idx], yd, g.zero_level, om);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) src_s[(s * EPB) * NP + idx] = (R)(c_mech.mw[s] * om[s]);
+        for (int s = 0; s < NS; ++s) src_s[(s * EPB) * NP + idx] = (R)c_mech.mw[s] * om[s];
       }
     }
   }
@@ -669,7 +688,9 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
 #pragma unroll
     for (int c = 0; c < NC; ++c) qm[c] = q_s[(c * EPB + e) * NP + k];
     NodeState<R, DIM, NS> sm, sp;
-    make_state<R, DIM, NS>(qm, MIX ? t_s[e * NP + k] : R(0), g, sm);
+    // own side: the inviscid flux needs q, p, c, gamma only, kept from phase 2
+    make_state_light<R, DIM, NS>(qm, pcg_s[e * NP + k], pcg_s[EPB * NP + e * NP + k],
+                                 pcg_s[2 * EPB * NP + e * NP + k], sm);
     // own total flux . n from the metric-combined volume flux:
     // F.n = (sum_r N_r G_r) / |rx^T N|
     R nmag2 = R(0);
@@ -819,6 +840,355 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
           if (i >= NP) continue;
           R v = d[t][2 * half + h];
           if (sources && c >= 2 + DIM) v += src_s[((c - 2 - DIM) * EPB + e) * NP + i];
+          outp[i] = v;
+          bad |= !(v == v);
+        }
+    }
+  }
+  if (bad) atomicOr(a.status, ST_NAN);
+}
+
+// }}}
+
+// {{{ split right-hand side: pointwise flux kernel + surface/lift kernel
+//
+// k_node_flux evaluates every node's state and total flux F = F_V - F_I once
+// (plus p, c, gamma and the Arrhenius sources) and writes a flux record per
+// node.  k_surface then builds, per element tile, the metric-combined volume
+// terms from the records, the numerical face fluxes from the records of both
+// sides of each face node (the neighbour's flux is gathered, not
+// recomputed), and contracts on the tensor cores exactly as k_rhs does.
+// The split trades one record write + read per node for the 2-3x repeated
+// neighbour-state evaluations of the fused kernel.
+
+template <class R, int DIM, int ORDER, int NS, bool MIX, bool VISC>
+__global__ void __launch_bounds__(128, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_NODE))
+    k_node_flux(DGArgs<R> a, GasParams g) {
+  using C = Cfg<R, DIM, ORDER, NS, MIX>;
+  constexpr int NP = C::NP, NC = C::NC, FW = C::FW;
+  const int64_t EN = (int64_t)a.nelem * NP;
+  const bool sources = MIX && a.add_sources;
+  bool bad = false;
+  for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < EN;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    R qq[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) qq[c] = a.q[c * EN + n];
+    NodeState<R, DIM, NS> st;
+    make_state<R, DIM, NS>(qq, MIX ? a.t_op[n] : R(0), g, st);
+    R fl[NC][DIM];
+    inviscid_flux<R, DIM, NS>(st, fl);
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int j = 0; j < DIM; ++j) fl[c][j] = -fl[c][j];
+    if (VISC) {
+      R gqv[NC][DIM], gt[DIM];
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) gqv[c][j] = a.grad[((int64_t)c * DIM + j) * EN + n];
+#pragma unroll
+      for (int j = 0; j < DIM; ++j) gt[j] = a.grad[((int64_t)NC * DIM + j) * EN + n];
+      R fv[NC][DIM];
+      viscous_flux<R, DIM, NS, MIX>(st, gqv, gt, fv);
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) fl[c][j] = fv[c][j] + fl[c][j];
+    }
+    R rec[FW];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int j = 0; j < DIM; ++j) rec[c * DIM + j] = fl[c][j];
+    rec[NC * DIM] = st.p;
+    rec[NC * DIM + 1] = st.c;
+    rec[NC * DIM + 2] = st.gamma;
+#pragma unroll
+    for (int i = NC * DIM + 3; i < FW; ++i) rec[i] = R(0);
+    bad |= !(st.p == st.p) || !(st.c == st.c);
+    R* dst = a.fbuf + n * FW;
+    if constexpr (sizeof(R) == 4) {
+#pragma unroll
+      for (int i = 0; i < FW; i += 4)
+        *reinterpret_cast<float4*>(dst + i) = make_float4(rec[i], rec[i + 1], rec[i + 2], rec[i + 3]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < FW; i += 2)
+        *reinterpret_cast<double2*>(dst + i) = make_double2(rec[i], rec[i + 1]);
+    }
+    if constexpr (MIX && NS > 0) {
+      if (sources) {
+        R om[NS];
+        production_rates<R, NS>(st.rho, a.t_src[n], st.y, (R)g.zero_level, om);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) a.srcbuf[s * EN + n] = (R)c_mech.mw[s] * om[s];
+      }
+    }
+  }
+  if (bad) atomicOr(a.status, ST_NAN);
+}
+
+// flux record of one node into registers
+template <class R, int FW>
+__device__ __forceinline__ void load_record(const R* __restrict__ src, R (&rec)[FW]) {
+  if constexpr (sizeof(R) == 4) {
+#pragma unroll
+    for (int i = 0; i < FW; i += 4) {
+      const float4 v = *reinterpret_cast<const float4*>(src + i);
+      rec[i] = v.x;
+      rec[i + 1] = v.y;
+      rec[i + 2] = v.z;
+      rec[i + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < FW; i += 2) {
+      const double2 v = *reinterpret_cast<const double2*>(src + i);
+      rec[i] = v.x;
+      rec[i + 1] = v.y;
+    }
+  }
+}
+
+// Exterior state and its total flux . n on a prescribed boundary face node
+// (interior gradients on both sides, mirgecom/boundary.py:141-146).  Kept
+// out of line: it runs on boundary faces only and would otherwise inflate the
+// register allocation of the interior path.
+template <class R, int DIM, int NS, bool MIX, bool VISC>
+__device__ __noinline__ void prescribed_exterior_flux(const DGArgs<R>& a, const GasParams& g,
+                                                      const R* qp, R t_ext, int64_t gm,
+                                                      int64_t EN, const R* n,
+                                                      NodeState<R, DIM, NS>& sp, R* fpn) {
+  constexpr int NC = DIM + 2 + NS;
+  make_state<R, DIM, NS>(qp, t_ext, g, sp);
+  R fe[NC][DIM];
+  inviscid_flux<R, DIM, NS>(sp, fe);
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) fe[c][j] = -fe[c][j];
+  if (VISC) {
+    R gqp[NC][DIM], gtp[DIM];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int j = 0; j < DIM; ++j) gqp[c][j] = a.grad[((int64_t)c * DIM + j) * EN + gm];
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) gtp[j] = a.grad[((int64_t)NC * DIM + j) * EN + gm];
+    R fv[NC][DIM];
+    viscous_flux<R, DIM, NS, MIX>(sp, gqp, gtp, fv);
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int j = 0; j < DIM; ++j) fe[c][j] += fv[c][j];
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    R acc = R(0);
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) acc += fe[c][j] * n[j];
+    fpn[c] = acc;
+  }
+}
+
+template <class R, int DIM, int ORDER, int NS, bool MIX, bool VISC>
+__global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
+    k_surface(DGArgs<R> a, GasParams g) {
+  using C = Cfg<R, DIM, ORDER, NS, MIX>;
+  using S = Simplex<DIM, ORDER>;
+  constexpr int NP = C::NP, NF = C::NF, NFP = C::NFP, NFN = C::NFN, NC = C::NC, FW = C::FW;
+  constexpr int EPB = C::EPB_SURF, MP = C::MP, MT = C::MT, KB = C::KB, KR = C::KR;
+  constexpr int KRR = C::KRR, NCOL = C::NCOL_S;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* am = reinterpret_cast<R*>(smem_raw);                  // [NAC][MP][KB]
+  R* bm = am + C::NAC * MP * KB;                           // [NCOL][KB]
+  R* rx_s = bm + NCOL * KB;                                // [EPB][DIM][DIM]
+  R* nrm_s = rx_s + EPB * DIM * DIM;
+  R* fs_s = nrm_s + EPB * NF * DIM;
+  int* fn_s = reinterpret_cast<int*>(fs_s + EPB * NF);
+  uint8_t* perm_s = reinterpret_cast<uint8_t*>(fn_s + NFN);
+
+  const int E = a.nelem;
+  const int e0 = blockIdx.x * EPB;
+  const int ne = imin(EPB, E - e0);
+  const int64_t EN = (int64_t)E * NP;
+  const bool sources = MIX && a.add_sources;
+
+  for (int i = threadIdx.x; i < MP * KB; i += blockDim.x) {
+    const int row = i / KB, k = i % KB;
+    double v = 0.0;
+    if (row < NP && k < KR) {
+      if (k < DIM * NP) {
+        const int r = k / NP, kk = k % NP;
+        v = -c_ref64[S::OFF_W + (r * NP + row) * NP + kk];
+      } else {
+        v = c_ref64[S::OFF_LIFT + row * NFN + (k - DIM * NP)];
+      }
+    }
+    put_a<R>(am, MP * KB, i, v);
+  }
+  for (int i = threadIdx.x; i < NCOL * KB; i += blockDim.x) bm[i] = R(0);
+  for (int i = threadIdx.x; i < NFN; i += blockDim.x) fn_s[i] = c_face_nodes<DIM, ORDER>(i);
+  for (int i = threadIdx.x; i < a.nperm * NFP; i += blockDim.x) perm_s[i] = a.perm[i];
+  load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
+  __syncthreads();
+
+  // volume terms: G_r = sum_j (dr_r/dx_j) F_j, shifted by the node-0 value
+  for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
+    const int e = idx / NP, k = idx % NP;
+    R f[FW], f0[FW];
+    load_record<R, FW>(a.fbuf + ((int64_t)e0 * NP + idx) * FW, f);
+    load_record<R, FW>(a.fbuf + ((int64_t)(e0 + e) * NP) * FW, f0);
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int r = 0; r < DIM; ++r) {
+        R acc = R(0);
+#pragma unroll
+        for (int j = 0; j < DIM; ++j)
+          acc += rx_s[e * DIM * DIM + r * DIM + j] * (f[c * DIM + j] - f0[c * DIM + j]);
+        bm[(c * EPB + e) * KB + r * NP + k] = acc;
+      }
+  }
+
+  // numerical face fluxes from the records of both sides
+  for (int idx = threadIdx.x; idx < ne * NFN; idx += blockDim.x) {
+    const int e = idx / NFN, fm = idx % NFN, f = fm / NFP, m = fm % NFP;
+    const int k = fn_s[fm];
+    const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
+    const R fsc = fs_s[e * NF + f];
+    R n[DIM];
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) n[j] = nrm_s[(e * NF + f) * DIM + j];
+    const int64_t gm = (int64_t)(e0 + e) * NP + k;
+    R fr[FW], f0[FW];
+    load_record<R, FW>(a.fbuf + gm * FW, fr);
+    load_record<R, FW>(a.fbuf + ((int64_t)(e0 + e) * NP) * FW, f0);
+    R qm[NC], qp[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) qm[c] = a.q[c * EN + gm];
+    NodeState<R, DIM, NS> sm, sp;
+    make_state_light<R, DIM, NS>(qm, fr[NC * DIM], fr[NC * DIM + 1], fr[NC * DIM + 2], sm);
+    R ftm[NC], f0n[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      R acc = R(0), acc0 = R(0);
+#pragma unroll
+      for (int j = 0; j < DIM; ++j) {
+        acc += fr[c * DIM + j] * n[j];
+        acc0 += f0[c * DIM + j] * n[j];
+      }
+      ftm[c] = acc;
+      f0n[c] = acc0;
+    }
+    int mode = 0;   // 0 interior, 1 dummy (interior only), 2 prescribed exterior
+    R fpn[NC];
+    if (cn >= 0) {
+      const int en = cn >> 8, pr = cn & 255;
+      const int kn = (pr < a.nperm) ? perm_s[pr * NFP + m] : NP;
+      if (en >= E || kn >= NP) {
+        atomicOr(a.status, ST_BAD_INDEX);
+        mode = 1;
+      } else {
+        const int64_t gi = (int64_t)en * NP + kn;
+        load_record<R, FW>(a.fbuf + gi * FW, fr);     // reuse: neighbour record
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          qp[c] = a.q[c * EN + gi];
+          R acc = R(0);
+#pragma unroll
+          for (int j = 0; j < DIM; ++j) acc += fr[c * DIM + j] * n[j];
+          fpn[c] = acc;
+        }
+        make_state_light<R, DIM, NS>(qp, fr[NC * DIM], fr[NC * DIM + 1], fr[NC * DIM + 2], sp);
+      }
+    } else {
+      const int bf = -(cn + 1);
+      const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
+      if (kind == BK_PRESCRIBED) {
+        mode = 2;
+        const int64_t bstride = (int64_t)a.nbf * NFP;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) qp[c] = a.bext[c * bstride + (int64_t)bf * NFP + m];
+        prescribed_exterior_flux<R, DIM, NS, MIX, VISC>(
+            a, g, qp, MIX ? a.bext[NC * bstride + (int64_t)bf * NFP + m] : R(0), gm, EN, n, sp,
+            fpn);
+      } else {
+        if (kind < 0) atomicOr(a.status, ST_BAD_INDEX);
+        mode = 1;
+      }
+    }
+    R out[NC];
+    if (mode == 1) {
+      // DummyBoundary: F_V(q-).n - F_I(q-).n  (boundary.py:1027-1049)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) out[c] = ftm[c];
+    } else {
+      // F* = central(F_V) - numflux(F_I);  F_V.n = F.n + F_I.n on each side
+      R fi[NC], fim[NC], fip[NC];
+      inviscid_num_flux<R, DIM, NS>(sm, sp, qm, qp, n, a.flux_kind, fi);
+      inviscid_flux_n<R, DIM, NS>(sm, n, fim);
+      inviscid_flux_n<R, DIM, NS>(sp, n, fip);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        out[c] = -fi[c];
+        if (VISC) out[c] += ((ftm[c] + fim[c]) + (fpn[c] + fip[c])) / R(2);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) bm[(c * EPB + e) * KB + DIM * NP + fm] = fsc * (out[c] - f0n[c]);
+  }
+  __syncthreads();
+
+  // rhs = [-W | LIFT] [G ; S] on the tensor cores (+ sources)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gq = lane >> 2, tq = lane & 3;
+  constexpr int NACC = C::TF32 ? 4 : 2;
+  bool bad = false;
+  for (int nt = warp; nt < NCOL / 8; nt += blockDim.x >> 5) {
+    R d[MT][NACC];
+#pragma unroll
+    for (int t = 0; t < MT; ++t)
+#pragma unroll
+      for (int v = 0; v < NACC; ++v) d[t][v] = R(0);
+    const R* bcol = bm + (nt * 8 + gq) * KB + tq;
+    if constexpr (!C::TF32) {
+#pragma unroll 5
+      for (int ks = 0; ks < KRR / 4; ++ks) {
+        const double b = bcol[ks * 4];
+#pragma unroll
+        for (int t = 0; t < MT; ++t) dmma884(d[t], am[(t * 8 + gq) * KB + ks * 4 + tq], b);
+      }
+    } else {
+#pragma unroll 2
+      for (int ks = 0; ks < KRR / 8; ++ks) {
+        const float b0 = bcol[ks * 8], b1 = bcol[ks * 8 + 4];
+#pragma unroll
+        for (int t = 0; t < MT; ++t) {
+          uint32_t ah[4], alo[4];
+          load_a_tf32(ah, am, KB, t * 16, ks * 8, gq, tq);
+          load_a_tf32(alo, am + MP * KB, KB, t * 16, ks * 8, gq, tq);
+          mma_tf32x3(d[t], ah, alo, b0, b1);
+        }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int col = nt * 8 + 2 * tq + h;
+      const int c = col / EPB, e = col % EPB;
+      if (c >= NC || e >= ne) continue;
+      R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
+#pragma unroll
+      for (int t = 0; t < MT; ++t)
+#pragma unroll
+        for (int half = 0; half < NACC / 2; ++half) {
+          const int i = t * Tile<R>::MROW + gq + 8 * half;
+          if (i >= NP) continue;
+          R v = d[t][2 * half + h];
+          if (sources && c >= 2 + DIM)
+            v += a.srcbuf[(int64_t)(c - 2 - DIM) * EN + (int64_t)(e0 + e) * NP + i];
           outp[i] = v;
           bad |= !(v == v);
         }

@@ -27,6 +27,10 @@ int tu3f_mixture_state(int, int64_t, const float*, const float*, const float*, f
                        int, float, int32_t*, const GasParams&, cudaStream_t);
 int tu3_mixture_state(int, int64_t, const double*, const double*, double*, double*,
                       const GasParams&, cudaStream_t);
+size_t tu2_split_workspace(int, int, bool, int64_t);
+size_t tu3_split_workspace(int, int, bool, int64_t);
+size_t tu2f_split_workspace(int, int, bool, int64_t);
+size_t tu3f_split_workspace(int, int, bool, int64_t);
 }  // namespace mgc
 
 using namespace mgc;
@@ -158,9 +162,69 @@ int ns_rhs_impl(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const R* q, const 
   return dispatch(2, mesh, gas, a, (cudaStream_t)stream);
 }
 
+template <class R>
+size_t split_ws(const mgc_mesh_t* m, const mgc_gas_t* g) {
+  const bool mix = g->eos_kind == MGC_EOS_MIXTURE;
+  if constexpr (sizeof(R) == 8)
+    return m->dim == 2 ? tu2_split_workspace(m->order, g->nspecies, mix, m->nelem)
+                       : tu3_split_workspace(m->order, g->nspecies, mix, m->nelem);
+  return m->dim == 2 ? tu2f_split_workspace(m->order, g->nspecies, mix, m->nelem)
+                     : tu3f_split_workspace(m->order, g->nspecies, mix, m->nelem);
+}
+
+template <class R>
+int rhs_split_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const R* q,
+                   const R* t_op, const R* t_src, const R* grad, const R* bext, int flux_kind,
+                   int add_sources, R* rhs, void* workspace, size_t workspace_bytes,
+                   int32_t* status, void* stream) {
+  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !rhs || !status || !workspace)
+    return MGC_E_INVALID;
+  if (visc && !grad) return MGC_E_INVALID;
+  if (flux_kind < 0 || flux_kind > 2) return MGC_E_INVALID;
+  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
+  if (add_sources && (gas->eos_kind != MGC_EOS_MIXTURE || !t_src)) return MGC_E_INVALID;
+  if (reinterpret_cast<uintptr_t>(workspace) % 16) return MGC_E_INVALID;
+  int rc = ready(mesh, gas);
+  if (rc) return rc;
+  const size_t need = split_ws<R>(mesh, gas);
+  if (need == 0) return MGC_E_UNSUPPORTED;
+  if (workspace_bytes < need) return MGC_E_INVALID;
+  DGArgs<R> a = make_args<R>(mesh, q, t_op, t_src, grad, rhs, bext, flux_kind, add_sources,
+                             status);
+  a.fbuf = static_cast<R*>(workspace);
+  // sources after the flux records, 16-byte aligned
+  const size_t rec_bytes = need - 256 - (size_t)gas->nspecies * mesh->nelem *
+                                            mgc::simplex_npts(mesh->dim, mesh->order) * sizeof(R);
+  a.srcbuf = reinterpret_cast<R*>(static_cast<char*>(workspace) + ((rec_bytes + 15) / 16) * 16);
+  return dispatch(visc ? 4 : 3, mesh, gas, a, (cudaStream_t)stream);
+}
+
 }  // namespace
 
 extern "C" {
+
+size_t mgc_rhs_split_workspace_bytes(const mgc_mesh_t* mesh, const mgc_gas_t* gas,
+                                     int single_precision) {
+  if (!mesh_ok(mesh) || !gas_ok(gas)) return 0;
+  return single_precision ? split_ws<float>(mesh, gas) : split_ws<double>(mesh, gas);
+}
+
+int mgc_rhs_split(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
+                  const double* t_op, const double* t_src, const double* grad,
+                  const double* bext, int flux_kind, int add_sources, double* rhs,
+                  void* workspace, size_t workspace_bytes, int32_t* status, void* stream) {
+  return rhs_split_impl<double>(viscous, mesh, gas, q, t_op, t_src, grad, bext, flux_kind,
+                                add_sources, rhs, workspace, workspace_bytes, status, stream);
+}
+
+int mgc_rhs_split_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
+                      const float* t_op, const float* t_src, const float* grad,
+                      const float* bext, int flux_kind, int add_sources, float* rhs,
+                      void* workspace, size_t workspace_bytes, int32_t* status, void* stream) {
+  return rhs_split_impl<float>(viscous, mesh, gas, q, t_op, t_src, grad, bext, flux_kind,
+                               add_sources, rhs, workspace, workspace_bytes, status, stream);
+}
+
 
 int mgc_version(void) { return 1; }
 
@@ -214,8 +278,7 @@ int mgc_set_mechanism(const mgc_mechanism_t* mech_host) {
   if (!mech_host || mech_host->nspecies < 1 || mech_host->nspecies > MGC_MAX_SPECIES ||
       mech_host->nreactions < 0 || mech_host->nreactions > MGC_MAX_REACTIONS)
     return MGC_E_INVALID;
-  Mechanism m;
-  std::memcpy(&m, mech_host, sizeof(m));
+  const Mechanism m = expand_mechanism(*mech_host);
   int rc = tu2_upload_mechanism(&m);
   if (rc) return rc;
   rc = tu3_upload_mechanism(&m);

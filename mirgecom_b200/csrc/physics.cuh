@@ -58,6 +58,10 @@ struct Mechanism {
   double beta[MGC_MAX_REACTIONS];
   double t_act[MGC_MAX_REACTIONS];
   int32_t reversible[MGC_MAX_REACTIONS];
+  // derived at upload: enthalpy coefficients (a0, a1/2, a2/3, a3/4, a4/5, a5)
+  // and entropy coefficients (a0, a1, a2/2, a3/3, a4/4, a6), low / high range
+  double h_lo[MGC_MAX_SPECIES][6], h_hi[MGC_MAX_SPECIES][6];
+  double s_lo[MGC_MAX_SPECIES][6], s_hi[MGC_MAX_SPECIES][6];
 };
 
 // one copy per translation unit, filled by mgc_set_mechanism()
@@ -80,47 +84,60 @@ template <> __device__ __forceinline__ float rsqrt_<float>(float x) { return rsq
 
 // {{{ NASA-7 thermochemistry
 
-// a[k] for species s at temperature t (high range when t > t_mid)
+// Powers of T shared by every species of one NASA-7 evaluation.
 template <class R>
-__device__ __forceinline__ R nasa_coef(int s, int k, R t) {
-  return (R)((t > (R)c_mech.t_mid[s]) ? c_mech.a_hi[s][k] : c_mech.a_lo[s][k]);
+struct TPow {
+  R t, t2, t3, t4, it;
+  __device__ __forceinline__ explicit TPow(R tt)
+      : t(tt), t2(tt * tt), t3(tt * tt * tt), t4(tt * tt * tt * tt), it(R(1) / tt) {}
+};
+
+// cp/R and h/RT of species s (high range when t > t_mid)
+template <class R>
+__device__ __forceinline__ void nasa_cp_h(int s, const TPow<R>& p, R& cp, R& h) {
+  const bool hi = p.t > (R)c_mech.t_mid[s];
+  const double* a = hi ? c_mech.a_hi[s] : c_mech.a_lo[s];
+  const double* b = hi ? c_mech.h_hi[s] : c_mech.h_lo[s];
+  cp = (R)a[0] + (R)a[1] * p.t + (R)a[2] * p.t2 + (R)a[3] * p.t3 + (R)a[4] * p.t4;
+  h = (R)b[0] + (R)b[1] * p.t + (R)b[2] * p.t2 + (R)b[3] * p.t3 + (R)b[4] * p.t4 +
+      (R)b[5] * p.it;
 }
 
 template <class R>
 __device__ __forceinline__ R species_cp_r(int s, R t) {
-  const R a0 = nasa_coef<R>(s, 0, t), a1 = nasa_coef<R>(s, 1, t),
-          a2 = nasa_coef<R>(s, 2, t), a3 = nasa_coef<R>(s, 3, t),
-          a4 = nasa_coef<R>(s, 4, t);
-  return a0 + a1 * t + a2 * t * t + a3 * t * t * t + a4 * t * t * t * t;
+  R cp, h;
+  nasa_cp_h<R>(s, TPow<R>(t), cp, h);
+  return cp;
 }
 
 template <class R>
 __device__ __forceinline__ R species_h_rt(int s, R t) {
-  const R a0 = nasa_coef<R>(s, 0, t), a1 = nasa_coef<R>(s, 1, t),
-          a2 = nasa_coef<R>(s, 2, t), a3 = nasa_coef<R>(s, 3, t),
-          a4 = nasa_coef<R>(s, 4, t), a5 = nasa_coef<R>(s, 5, t);
-  return a0 + a1 / (R)2 * t + a2 / (R)3 * t * t + a3 / (R)4 * t * t * t +
-         a4 / (R)5 * t * t * t * t + a5 / t;
+  R cp, h;
+  nasa_cp_h<R>(s, TPow<R>(t), cp, h);
+  return h;
 }
 
+// s/R of species s given log(t)
 template <class R>
-__device__ __forceinline__ R species_s_r(int s, R t) {
-  const R a0 = nasa_coef<R>(s, 0, t), a1 = nasa_coef<R>(s, 1, t),
-          a2 = nasa_coef<R>(s, 2, t), a3 = nasa_coef<R>(s, 3, t),
-          a4 = nasa_coef<R>(s, 4, t), a6 = nasa_coef<R>(s, 6, t);
-  return a0 * log(t) + a1 * t + a2 / (R)2 * t * t + a3 / (R)3 * t * t * t +
-         a4 / (R)4 * t * t * t * t + a6;
+__device__ __forceinline__ R species_s_r(int s, const TPow<R>& p, R logt) {
+  const bool hi = p.t > (R)c_mech.t_mid[s];
+  const double* c = hi ? c_mech.s_hi[s] : c_mech.s_lo[s];
+  return (R)c[0] * logt + (R)c[1] * p.t + (R)c[2] * p.t2 + (R)c[3] * p.t3 + (R)c[4] * p.t4 +
+         (R)c[5];
 }
 
 // mixture e (J/kg) and c_v (J/kg/K) at temperature t
 template <class R, int NS>
 __device__ __forceinline__ void mixture_e_cv(const R* y, R t, R& e, R& cv) {
+  const TPow<R> p(t);
   R se = 0, scv = 0;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
+    R cps, hs;
+    nasa_cp_h<R>(s, p, cps, hs);
     const R yw = y[s] * (R)c_mech.inv_mw[s];
-    se += yw * (species_h_rt<R>(s, t) - (R)1);
-    scv += yw * (species_cp_r<R>(s, t) - (R)1);
+    se += yw * (hs - (R)1);
+    scv += yw * (cps - (R)1);
   }
   e = (R)kGasConstant * t * se;
   cv = (R)kGasConstant * scv;
@@ -134,12 +151,36 @@ __device__ __forceinline__ R mixture_gas_const(const R* y) {
   return (R)kGasConstant * s;
 }
 
+// mixture c_p and the species enthalpies (J/kg) in one NASA-7 pass
 template <class R, int NS>
-__device__ __forceinline__ R mixture_cp(const R* y, R t) {
+__device__ __forceinline__ R mixture_cp_and_h(const R* y, R t, R* h) {
+  const TPow<R> p(t);
   R s = 0;
 #pragma unroll
-  for (int k = 0; k < NS; ++k) s += y[k] * species_cp_r<R>(k, t) * (R)c_mech.inv_mw[k];
+  for (int k = 0; k < NS; ++k) {
+    R cps, hs;
+    nasa_cp_h<R>(k, p, cps, hs);
+    s += y[k] * cps * (R)c_mech.inv_mw[k];
+    h[k] = ((R)kGasConstant * (R)c_mech.inv_mw[k]) * t * hs;
+  }
   return (R)kGasConstant * s;
+}
+
+template <class R, int NS>
+__device__ __forceinline__ R mixture_cp(const R* y, R t) {
+  R h[NS];
+  return mixture_cp_and_h<R, NS>(y, t, h);
+}
+
+// c^o for a concentration c >= 0 and a positive order o
+template <class R>
+__device__ __forceinline__ R conc_pow(R c, R o) {
+  if (o == R(1)) return c;
+  if constexpr (sizeof(R) == 4) {
+    return c > 0.f ? expf(o * logf(c)) : 0.f;
+  } else {
+    return pow(c, o);
+  }
 }
 
 // T_{i+1} = T_i + (e - e(T_i)) / c_v(T_i), fixed count
@@ -167,13 +208,14 @@ __device__ __forceinline__ void production_rates(R rho, R t, const R* y, R zero_
   }
   const R logt = log(t);
   const R invt = (R)1 / t;
+  const TPow<R> tp(t);
   for (int i = 0; i < c_mech.nreactions; ++i) {
     const R kf = exp((R)c_mech.log_a[i] + (R)c_mech.beta[i] * logt - (R)c_mech.t_act[i] * invt);
     R rf = kf;
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
       const R o = (R)c_mech.ord_f[i][k];
-      if (o != (R)0) rf = rf * ((o == (R)1) ? conc[k] : pow(conc[k], o));
+      if (o != (R)0) rf = rf * conc_pow<R>(conc[k], o);
     }
     R r = rf;
     if (c_mech.reversible[i]) {
@@ -181,14 +223,18 @@ __device__ __forceinline__ void production_rates(R rho, R t, const R* y, R zero_
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
         const R nu = (R)c_mech.nu_net[i][k];
-        if (nu != (R)0) dg += nu * (species_h_rt<R>(k, t) - species_s_r<R>(k, t));
+        if (nu != (R)0) {
+          R cps, hs;
+          nasa_cp_h<R>(k, tp, cps, hs);
+          dg += nu * (hs - species_s_r<R>(k, tp, logt));
+        }
       }
       const R log_kc = -dg + (R)c_mech.dnu[i] * log((R)kOneAtm / ((R)kGasConstant * t));
       R rr = kf * exp(-log_kc);
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
         const R o = (R)c_mech.nu_p[i][k];
-        if (o != (R)0) rr = rr * ((o == (R)1) ? conc[k] : pow(conc[k], o));
+        if (o != (R)0) rr = rr * conc_pow<R>(conc[k], o);
       }
       r = rf - rr;
     }
@@ -246,13 +292,10 @@ __device__ __forceinline__ void make_state(const R* q, R t_in, const GasParams& 
       s.t = t_in;
       const R rmix = mixture_gas_const<R, NS>(s.y);
       s.p = s.rho * rmix * s.t;
-      const R cp = mixture_cp<R, NS>(s.y, s.t);
+      const R cp = mixture_cp_and_h<R, NS>(s.y, s.t, s.h);
       s.gamma = cp / (cp - rmix);
       s.cv = cp - rmix;
       s.c = sqrt(s.gamma * s.p / s.rho);
-#pragma unroll
-      for (int k = 0; k < NS; ++k)
-        s.h[k] = ((R)kGasConstant * (R)c_mech.inv_mw[k]) * s.t * species_h_rt<R>(k, s.t);
     }
   }
   // transport
@@ -275,6 +318,25 @@ __device__ __forceinline__ void make_state(const R* q, R t_in, const GasParams& 
 #pragma unroll
     for (int k = 0; k < NS; ++k) s.d[k] = 0;
   }
+}
+
+// Inviscid-only state from q and the node's p, c, gamma (computed before by
+// make_state): all the numerical inviscid fluxes need.
+template <class R, int DIM, int NS>
+__device__ __forceinline__ void make_state_light(const R* q, R p, R c, R gamma,
+                                                 NodeState<R, DIM, NS>& s) {
+  s.rho = q[0];
+  s.rhoe = q[1];
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) {
+    s.mom[i] = q[2 + i];
+    s.v[i] = s.mom[i] / s.rho;
+  }
+#pragma unroll
+  for (int k = 0; k < NS; ++k) s.rhoy[k] = q[2 + DIM + k];
+  s.p = p;
+  s.c = c;
+  s.gamma = gamma;
 }
 
 // Temperature of a node from q (ideal: closed form; mixture: Newton from seed)

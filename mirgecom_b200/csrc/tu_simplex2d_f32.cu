@@ -28,4 +28,14 @@ int tu2f_mixture_state(int ns, int64_t nnodes, const float* q, const float* tsee
                                        status, g, s);
 }
 
+size_t tu2f_split_workspace(int order, int ns, bool mix, int64_t nelem) {
+  switch (order) {
+    case 1: return split_workspace_order<float, 2, 1>(ns, mix, nelem);
+    case 2: return split_workspace_order<float, 2, 2>(ns, mix, nelem);
+    case 3: return split_workspace_order<float, 2, 3>(ns, mix, nelem);
+    case 4: return split_workspace_order<float, 2, 4>(ns, mix, nelem);
+    default: return 0;
+  }
+}
+
 }  // namespace mgc

@@ -25,4 +25,14 @@ int tu2_mixture_state(int ns, int64_t nnodes, const double* q, const double* tse
   return mixture_state_dim<double, 2>(ns, nnodes, q, tseed, t1, t2, g, s);
 }
 
+size_t tu2_split_workspace(int order, int ns, bool mix, int64_t nelem) {
+  switch (order) {
+    case 1: return split_workspace_order<double, 2, 1>(ns, mix, nelem);
+    case 2: return split_workspace_order<double, 2, 2>(ns, mix, nelem);
+    case 3: return split_workspace_order<double, 2, 3>(ns, mix, nelem);
+    case 4: return split_workspace_order<double, 2, 4>(ns, mix, nelem);
+    default: return 0;
+  }
+}
+
 }  // namespace mgc

@@ -27,4 +27,13 @@ int tu3f_mixture_state(int ns, int64_t nnodes, const float* q, const float* tsee
                                        status, g, s);
 }
 
+size_t tu3f_split_workspace(int order, int ns, bool mix, int64_t nelem) {
+  switch (order) {
+    case 1: return split_workspace_order<float, 3, 1>(ns, mix, nelem);
+    case 2: return split_workspace_order<float, 3, 2>(ns, mix, nelem);
+    case 3: return split_workspace_order<float, 3, 3>(ns, mix, nelem);
+    default: return 0;
+  }
+}
+
 }  // namespace mgc

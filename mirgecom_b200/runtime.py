@@ -207,6 +207,19 @@ def _operator_temperature(state):
     return state.operator_temperature.contiguous()
 
 
+# The divergence pass runs split (pointwise flux records + surface/lift
+# kernel) by default; the fused single-kernel form stays available.
+SPLIT_RHS = True
+
+
+def _split_workspace(dd, gs, f32):
+    lib = _lib.load()
+    nbytes = lib.mgc_rhs_split_workspace_bytes(C.byref(dd.mesh), C.byref(gs), int(f32))
+    if nbytes == 0:
+        raise RuntimeError("split right-hand side unsupported for this configuration")
+    return dd.workspace("split_ws", ((nbytes + 15) // 16 * 16,), torch.uint8)
+
+
 def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
     q = state.cv.q
     _lib.require_cuda(q)
@@ -219,7 +232,17 @@ def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
     bext = boundary_exterior(dd, state, gas_model, boundaries, time)
     t_op = _operator_temperature(state)
     rhs = torch.empty_like(q)
-    fn = lib.mgc_euler_rhs_f32 if q.dtype == torch.float32 else lib.mgc_euler_rhs
+    f32 = q.dtype == torch.float32
+    if SPLIT_RHS:
+        ws = _split_workspace(dd, gs, f32)
+        fsplit = lib.mgc_rhs_split_f32 if f32 else lib.mgc_rhs_split
+        with torch.cuda.device(q.device):
+            _lib.check(fsplit(0, C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op),
+                              None, None, _lib.ptr(bext), flux_kind, 0, _lib.ptr(rhs),
+                              _lib.ptr(ws), ws.numel(), _lib.ptr(dd.status),
+                              _lib.stream_handle()), "mgc_rhs_split")
+        return rhs
+    fn = lib.mgc_euler_rhs_f32 if f32 else lib.mgc_euler_rhs
     with torch.cuda.device(q.device):
         _lib.check(fn(
             C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(bext),
@@ -262,10 +285,18 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
             _lib.ptr(grad), _lib.ptr(dd.status), stream), "mgc_ns_grad")
         if events:
             events[1].record()
-        _lib.check(frhs(
-            C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(t_src),
-            _lib.ptr(grad), _lib.ptr(bext), flux_kind, int(add_src), _lib.ptr(rhs),
-            _lib.ptr(dd.status), stream), "mgc_ns_rhs")
+        if SPLIT_RHS:
+            ws = _split_workspace(dd, gs, f32)
+            fsplit = lib.mgc_rhs_split_f32 if f32 else lib.mgc_rhs_split
+            _lib.check(fsplit(1, C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op),
+                              _lib.ptr(t_src), _lib.ptr(grad), _lib.ptr(bext), flux_kind,
+                              int(add_src), _lib.ptr(rhs), _lib.ptr(ws), ws.numel(),
+                              _lib.ptr(dd.status), stream), "mgc_rhs_split")
+        else:
+            _lib.check(frhs(
+                C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(t_src),
+                _lib.ptr(grad), _lib.ptr(bext), flux_kind, int(add_src), _lib.ptr(rhs),
+                _lib.ptr(dd.status), stream), "mgc_ns_rhs")
         if events:
             events[2].record()
     return rhs, grad

@@ -203,3 +203,51 @@ def test_uniform_state_rhs_zero(cuda, dim):
         rhs = euler_operator(d, make_fluid_state(_cv(q, dim, cuda), gas), gas,
                              {"all": DummyBoundary()}, inviscid_numerical_flux_func=flux)
         assert float(rhs.q.abs().max()) < 1e-9
+
+
+@pytest.mark.parametrize("case", ["tgv", "mixture", "boundaries_hll"])
+def test_split_and_fused_divergence_agree(cuda, case):
+    """The two-kernel (flux records + surface) and fused divergence passes."""
+    if case == "tgv":
+        d, od = make_disc("simplex", 3, 3, 3, (-np.pi,) * 3, (np.pi,) * 3, True)
+        q = tgv_np(od.nodes)
+        mu = 1.0 / 1600
+        gas = GasModel(eos=IdealSingleGas(), transport=SimpleTransport(
+            viscosity=mu, thermal_conductivity=mu * 1004.85 / 0.71))
+        st = make_fluid_state(_cv(q, 3, cuda), gas)
+        kw, bnds, flux = {}, {}, inviscid_facial_flux_rusanov
+    elif case == "mixture":
+        d, od = make_disc("simplex", 3, 3, 3, (0.0,) * 3, (2 * np.pi,) * 3, True)
+        from mirgecom_b200.initializers import reacting_mixture_state
+        cv0, t_true = reacting_mixture_state([torch.from_numpy(od.nodes[i]) for i in range(3)],
+                                             UIUC_7SP, seed=5)
+        gas = GasModel(eos=PyrometheusMixture(UIUC_7SP), transport=SimpleTransport(
+            viscosity=1e-5, thermal_conductivity=2e-5, species_diffusivity=[1e-5] * 7))
+        st = make_fluid_state(ConservedVars(cv0.q.to(cuda), 3), gas,
+                              temperature_seed=t_true.to(cuda) + 10.0)
+        kw, bnds, flux = {"species_source_temperature": st.temperature}, {}, \
+            inviscid_facial_flux_rusanov
+    else:
+        d, od = make_disc("simplex", 2, 5, 2, (0.0, 0.0), (2.0, 1.0), False)
+        q = perturbed_state_np(od.nodes, 2, 2, seed=3)
+        gas = GasModel(eos=IdealSingleGas(), transport=PowerLawTransport(
+            species_diffusivity=[1e-2, 2e-2], beta=1e-2))
+
+        def bnd(dcoll, dd_bdry, gas_model, state_minus, time, nodes, **k):
+            return make_fluid_state(_cv(perturbed_state_np(nodes.cpu().numpy(), 2, 2, seed=4),
+                                        2, cuda), gas_model)
+
+        bnds = {"-0": DummyBoundary(), "+0": PrescribedFluidBoundary(boundary_state_func=bnd),
+                "-1": PrescribedFluidBoundary(boundary_state_func=bnd), "+1": DummyBoundary()}
+        st = make_fluid_state(_cv(q, 2, cuda), gas)
+        kw, flux = {}, inviscid_facial_flux_hll
+    outs = {}
+    for split in (True, False):
+        runtime.SPLIT_RHS = split
+        try:
+            outs[split] = ns_operator(d, gas, st, bnds, inviscid_numerical_flux_func=flux,
+                                      **kw).q.cpu().numpy()
+        finally:
+            runtime.SPLIT_RHS = True
+    assert field_rel_l2(outs[True], outs[False]) < TOL
+    _status_ok(d)
