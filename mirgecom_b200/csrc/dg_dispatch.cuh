@@ -39,6 +39,12 @@ inline Mechanism expand_mechanism(const mgc_mechanism_t& m) {
   return d;
 }
 
+// The helpers below touch this translation unit's own constant banks and
+// kernels, so they have internal linkage: a shared (inline, external) copy
+// could be kept by the linker from any one unit and would then upload to,
+// or launch from, that unit only.
+namespace {
+
 inline int upload_refops_local(int dim, int order, const double* packed64, const float* packed32,
                                const int* fnodes) {
   const int off = refops_offset(dim, order);
@@ -55,8 +61,40 @@ inline int upload_refops_local(int dim, int order, const double* packed64, const
   return MGC_OK;
 }
 
+// float copy of the device mechanism (every coefficient rounded to nearest)
+inline MechanismT<float> narrow_mechanism(const Mechanism& d) {
+  MechanismT<float> f;
+  memset(&f, 0, sizeof(f));
+  f.nspecies = d.nspecies;
+  f.nreactions = d.nreactions;
+  auto cp = [](float* dst, const double* src, int n) {
+    for (int i = 0; i < n; ++i) dst[i] = (float)src[i];
+  };
+  constexpr int S = MGC_MAX_SPECIES, R = MGC_MAX_REACTIONS;
+  cp(f.mw, d.mw, S);
+  cp(f.inv_mw, d.inv_mw, S);
+  cp(f.t_mid, d.t_mid, S);
+  cp(&f.a_lo[0][0], &d.a_lo[0][0], S * 7);
+  cp(&f.a_hi[0][0], &d.a_hi[0][0], S * 7);
+  cp(&f.ord_f[0][0], &d.ord_f[0][0], R * S);
+  cp(&f.nu_p[0][0], &d.nu_p[0][0], R * S);
+  cp(&f.nu_net[0][0], &d.nu_net[0][0], R * S);
+  cp(f.dnu, d.dnu, R);
+  cp(f.log_a, d.log_a, R);
+  cp(f.beta, d.beta, R);
+  cp(f.t_act, d.t_act, R);
+  for (int i = 0; i < R; ++i) f.reversible[i] = d.reversible[i];
+  cp(&f.h_lo[0][0], &d.h_lo[0][0], S * 6);
+  cp(&f.h_hi[0][0], &d.h_hi[0][0], S * 6);
+  cp(&f.s_lo[0][0], &d.s_lo[0][0], S * 6);
+  cp(&f.s_hi[0][0], &d.s_hi[0][0], S * 6);
+  return f;
+}
+
 inline int upload_mechanism_local(const Mechanism* m) {
-  return cudaMemcpyToSymbol(c_mech, m, sizeof(Mechanism)) == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+  if (cudaMemcpyToSymbol(c_mech, m, sizeof(Mechanism)) != cudaSuccess) return MGC_E_CUDA;
+  const MechanismT<float> f = narrow_mechanism(*m);
+  return cudaMemcpyToSymbol(c_mech32, &f, sizeof(f)) == cudaSuccess ? MGC_OK : MGC_E_CUDA;
 }
 
 template <class Kern>
@@ -188,5 +226,7 @@ inline int mixture_state_dim(int ns, int64_t nnodes, const R* q, const R* tseed,
   k_mixture_state<R, DIM, 7><<<(unsigned)nb, nt, 0, s>>>(nnodes, q, tseed, t1, t2, g);
   return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
 }
+
+}  // namespace
 
 }  // namespace mgc

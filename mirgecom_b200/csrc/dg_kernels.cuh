@@ -228,6 +228,12 @@ __device__ __forceinline__ void load_a_tf32(uint32_t (&a)[4], const float* am, i
   a[3] = __float_as_uint(am[(m0 + g + 8) * stride + k0 + t + 4]);
 }
 
+// Everything below has internal linkage: every translation unit that
+// includes this file launches its own copies of the kernels, which read that
+// unit's constant banks.  (With external linkage the host linker may keep one
+// unit's launch stub for an instantiation that two units share.)
+namespace {
+
 // Per-element geometry: rx copy, unit normals and face factors derived from rx
 // (n dS = J rx^T N dS_ref;  fscale = |rx^T N| * face_scale_ref).
 template <class R, int DIM, int ORDER>
@@ -300,17 +306,18 @@ __global__ void __launch_bounds__(256) k_mixture_state_mixed(
     float qq[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) qq[c] = q[(int64_t)c * nnodes + n];
+    const double irho = 1.0 / (double)qq[0];
     float y[NS];
     double yd[NS];
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-      y[k] = qq[2 + DIM + k] / qq[0];
-      yd[k] = (double)qq[2 + DIM + k] / (double)qq[0];
+      yd[k] = (double)qq[2 + DIM + k] * irho;
+      y[k] = (float)yd[k];
     }
     double ked = 0;
 #pragma unroll
     for (int i = 0; i < DIM; ++i) ked += (double)qq[2 + i] * (double)qq[2 + i];
-    const double e64 = ((double)qq[1] - 0.5 * ked / (double)qq[0]) / (double)qq[0];
+    const double e64 = ((double)qq[1] - 0.5 * ked * irho) * irho;
     const float e32 = (float)e64;
     int used = 0;
     float t = 0.f;
@@ -669,7 +676,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
         R om[NS];
         production_rates<R, NS>(st.rho, t_s[EPB * NP + idx], st.y, (R)g.zero_level, om);
 #pragma unroll
-        for (int s = 0; s < NS; ++s) src_s[(s * EPB) * NP + idx] = (R)c_mech.mw[s] * om[s];
+        for (int s = 0; s < NS; ++s) src_s[(s * EPB) * NP + idx] = mech<R>().mw[s] * om[s];
       }
     }
   }
@@ -923,7 +930,7 @@ __global__ void __launch_bounds__(128, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_NODE))
         R om[NS];
         production_rates<R, NS>(st.rho, a.t_src[n], st.y, (R)g.zero_level, om);
 #pragma unroll
-        for (int s = 0; s < NS; ++s) a.srcbuf[s * EN + n] = (R)c_mech.mw[s] * om[s];
+        for (int s = 0; s < NS; ++s) a.srcbuf[s * EN + n] = mech<R>().mw[s] * om[s];
       }
     }
   }
@@ -1232,7 +1239,7 @@ __global__ void k_rk4_stage(int64_t n, const double* __restrict__ q0, const doub
 
 // mixed form: k arrives in float32, the state and the sum stay float64, and
 // the float32 copy of the new state feeds the next right-hand side
-static __global__ void k_rk4_stage_mixed(int64_t n, const double* __restrict__ q0,
+__global__ void k_rk4_stage_mixed(int64_t n, const double* __restrict__ q0,
                                   const float* __restrict__ k, double* __restrict__ sum,
                                   double* __restrict__ qout, float* __restrict__ qout_lo,
                                   int stage, double dt) {
@@ -1258,5 +1265,7 @@ static __global__ void k_rk4_stage_mixed(int64_t n, const double* __restrict__ q
 }
 
 // }}}
+
+}  // namespace
 
 }  // namespace mgc

@@ -42,30 +42,40 @@ struct GasParams {
   double zero_level;        // concentration floor
 };
 
-// Mechanism tables (SI units), uploaded once.
-struct Mechanism {
+// Mechanism tables (SI units), uploaded once.  T is the coefficient type:
+// the float64 kernels read MechanismT<double>, the float32 ones a float copy
+// (each coefficient rounded once on the host), so no kernel converts
+// coefficients at run time.
+template <class T>
+struct MechanismT {
   int32_t nspecies, nreactions;
-  double mw[MGC_MAX_SPECIES];
-  double inv_mw[MGC_MAX_SPECIES];
-  double t_mid[MGC_MAX_SPECIES];
-  double a_lo[MGC_MAX_SPECIES][7];
-  double a_hi[MGC_MAX_SPECIES][7];
-  double ord_f[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
-  double nu_p[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
-  double nu_net[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
-  double dnu[MGC_MAX_REACTIONS];
-  double log_a[MGC_MAX_REACTIONS];
-  double beta[MGC_MAX_REACTIONS];
-  double t_act[MGC_MAX_REACTIONS];
+  T mw[MGC_MAX_SPECIES];
+  T inv_mw[MGC_MAX_SPECIES];
+  T t_mid[MGC_MAX_SPECIES];
+  T a_lo[MGC_MAX_SPECIES][7];
+  T a_hi[MGC_MAX_SPECIES][7];
+  T ord_f[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
+  T nu_p[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
+  T nu_net[MGC_MAX_REACTIONS][MGC_MAX_SPECIES];
+  T dnu[MGC_MAX_REACTIONS];
+  T log_a[MGC_MAX_REACTIONS];
+  T beta[MGC_MAX_REACTIONS];
+  T t_act[MGC_MAX_REACTIONS];
   int32_t reversible[MGC_MAX_REACTIONS];
   // derived at upload: enthalpy coefficients (a0, a1/2, a2/3, a3/4, a4/5, a5)
   // and entropy coefficients (a0, a1, a2/2, a3/3, a4/4, a6), low / high range
-  double h_lo[MGC_MAX_SPECIES][6], h_hi[MGC_MAX_SPECIES][6];
-  double s_lo[MGC_MAX_SPECIES][6], s_hi[MGC_MAX_SPECIES][6];
+  T h_lo[MGC_MAX_SPECIES][6], h_hi[MGC_MAX_SPECIES][6];
+  T s_lo[MGC_MAX_SPECIES][6], s_hi[MGC_MAX_SPECIES][6];
 };
+using Mechanism = MechanismT<double>;
 
-// one copy per translation unit, filled by mgc_set_mechanism()
-static __constant__ Mechanism c_mech;
+// one copy of each per translation unit, filled by mgc_set_mechanism()
+static __constant__ MechanismT<double> c_mech;
+static __constant__ MechanismT<float> c_mech32;
+
+template <class R> __device__ __forceinline__ const MechanismT<R>& mech();
+template <> __device__ __forceinline__ const MechanismT<double>& mech<double>() { return c_mech; }
+template <> __device__ __forceinline__ const MechanismT<float>& mech<float>() { return c_mech32; }
 
 constexpr double kGasConstant = 8314.46261815324;
 constexpr double kOneAtm = 101325.0;
@@ -92,15 +102,24 @@ struct TPow {
       : t(tt), t2(tt * tt), t3(tt * tt * tt), t4(tt * tt * tt * tt), it(R(1) / tt) {}
 };
 
-// cp/R and h/RT of species s (high range when t > t_mid)
+// cp/R and h/RT of species s (high range when t > t_mid).  Both ranges are
+// evaluated and the result selected: the coefficient addresses then depend
+// on the species only, so every lane of a warp reads the same constants
+// (a per-lane choice of table would serialise the constant-cache reads).
 template <class R>
 __device__ __forceinline__ void nasa_cp_h(int s, const TPow<R>& p, R& cp, R& h) {
-  const bool hi = p.t > (R)c_mech.t_mid[s];
-  const double* a = hi ? c_mech.a_hi[s] : c_mech.a_lo[s];
-  const double* b = hi ? c_mech.h_hi[s] : c_mech.h_lo[s];
-  cp = (R)a[0] + (R)a[1] * p.t + (R)a[2] * p.t2 + (R)a[3] * p.t3 + (R)a[4] * p.t4;
-  h = (R)b[0] + (R)b[1] * p.t + (R)b[2] * p.t2 + (R)b[3] * p.t3 + (R)b[4] * p.t4 +
-      (R)b[5] * p.it;
+  const MechanismT<R>& m = mech<R>();
+  const R* al = m.a_lo[s];
+  const R* ah = m.a_hi[s];
+  const R* bl = m.h_lo[s];
+  const R* bh = m.h_hi[s];
+  const R cpl = al[0] + al[1] * p.t + al[2] * p.t2 + al[3] * p.t3 + al[4] * p.t4;
+  const R cph = ah[0] + ah[1] * p.t + ah[2] * p.t2 + ah[3] * p.t3 + ah[4] * p.t4;
+  const R hl = bl[0] + bl[1] * p.t + bl[2] * p.t2 + bl[3] * p.t3 + bl[4] * p.t4 + bl[5] * p.it;
+  const R hh = bh[0] + bh[1] * p.t + bh[2] * p.t2 + bh[3] * p.t3 + bh[4] * p.t4 + bh[5] * p.it;
+  const bool hi = p.t > m.t_mid[s];
+  cp = hi ? cph : cpl;
+  h = hi ? hh : hl;
 }
 
 template <class R>
@@ -117,13 +136,15 @@ __device__ __forceinline__ R species_h_rt(int s, R t) {
   return h;
 }
 
-// s/R of species s given log(t)
+// s/R of species s given log(t) (both ranges evaluated, as in nasa_cp_h)
 template <class R>
 __device__ __forceinline__ R species_s_r(int s, const TPow<R>& p, R logt) {
-  const bool hi = p.t > (R)c_mech.t_mid[s];
-  const double* c = hi ? c_mech.s_hi[s] : c_mech.s_lo[s];
-  return (R)c[0] * logt + (R)c[1] * p.t + (R)c[2] * p.t2 + (R)c[3] * p.t3 + (R)c[4] * p.t4 +
-         (R)c[5];
+  const MechanismT<R>& m = mech<R>();
+  const R* cl = m.s_lo[s];
+  const R* ch = m.s_hi[s];
+  const R sl = cl[0] * logt + cl[1] * p.t + cl[2] * p.t2 + cl[3] * p.t3 + cl[4] * p.t4 + cl[5];
+  const R sh = ch[0] * logt + ch[1] * p.t + ch[2] * p.t2 + ch[3] * p.t3 + ch[4] * p.t4 + ch[5];
+  return p.t > m.t_mid[s] ? sh : sl;
 }
 
 // mixture e (J/kg) and c_v (J/kg/K) at temperature t
@@ -135,7 +156,7 @@ __device__ __forceinline__ void mixture_e_cv(const R* y, R t, R& e, R& cv) {
   for (int s = 0; s < NS; ++s) {
     R cps, hs;
     nasa_cp_h<R>(s, p, cps, hs);
-    const R yw = y[s] * (R)c_mech.inv_mw[s];
+    const R yw = y[s] * mech<R>().inv_mw[s];
     se += yw * (hs - (R)1);
     scv += yw * (cps - (R)1);
   }
@@ -147,7 +168,7 @@ template <class R, int NS>
 __device__ __forceinline__ R mixture_gas_const(const R* y) {
   R s = 0;
 #pragma unroll
-  for (int k = 0; k < NS; ++k) s += y[k] * (R)c_mech.inv_mw[k];
+  for (int k = 0; k < NS; ++k) s += y[k] * mech<R>().inv_mw[k];
   return (R)kGasConstant * s;
 }
 
@@ -160,8 +181,8 @@ __device__ __forceinline__ R mixture_cp_and_h(const R* y, R t, R* h) {
   for (int k = 0; k < NS; ++k) {
     R cps, hs;
     nasa_cp_h<R>(k, p, cps, hs);
-    s += y[k] * cps * (R)c_mech.inv_mw[k];
-    h[k] = ((R)kGasConstant * (R)c_mech.inv_mw[k]) * t * hs;
+    s += y[k] * cps * mech<R>().inv_mw[k];
+    h[k] = ((R)kGasConstant * mech<R>().inv_mw[k]) * t * hs;
   }
   return (R)kGasConstant * s;
 }
@@ -202,44 +223,44 @@ __device__ __forceinline__ void production_rates(R rho, R t, const R* y, R zero_
   R conc[NS];
 #pragma unroll
   for (int k = 0; k < NS; ++k) {
-    R c = (R)c_mech.inv_mw[k] * rho * y[k];
+    R c = mech<R>().inv_mw[k] * rho * y[k];
     conc[k] = (c < zero_level) ? (R)0 : c;
     omega[k] = 0;
   }
   const R logt = log(t);
   const R invt = (R)1 / t;
   const TPow<R> tp(t);
-  for (int i = 0; i < c_mech.nreactions; ++i) {
-    const R kf = exp((R)c_mech.log_a[i] + (R)c_mech.beta[i] * logt - (R)c_mech.t_act[i] * invt);
+  for (int i = 0; i < mech<R>().nreactions; ++i) {
+    const R kf = exp(mech<R>().log_a[i] + mech<R>().beta[i] * logt - mech<R>().t_act[i] * invt);
     R rf = kf;
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-      const R o = (R)c_mech.ord_f[i][k];
+      const R o = mech<R>().ord_f[i][k];
       if (o != (R)0) rf = rf * conc_pow<R>(conc[k], o);
     }
     R r = rf;
-    if (c_mech.reversible[i]) {
+    if (mech<R>().reversible[i]) {
       R dg = 0;
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
-        const R nu = (R)c_mech.nu_net[i][k];
+        const R nu = mech<R>().nu_net[i][k];
         if (nu != (R)0) {
           R cps, hs;
           nasa_cp_h<R>(k, tp, cps, hs);
           dg += nu * (hs - species_s_r<R>(k, tp, logt));
         }
       }
-      const R log_kc = -dg + (R)c_mech.dnu[i] * log((R)kOneAtm / ((R)kGasConstant * t));
+      const R log_kc = -dg + mech<R>().dnu[i] * log((R)kOneAtm / ((R)kGasConstant * t));
       R rr = kf * exp(-log_kc);
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
-        const R o = (R)c_mech.nu_p[i][k];
+        const R o = mech<R>().nu_p[i][k];
         if (o != (R)0) rr = rr * conc_pow<R>(conc[k], o);
       }
       r = rf - rr;
     }
 #pragma unroll
-    for (int k = 0; k < NS; ++k) omega[k] += (R)c_mech.nu_net[i][k] * r;
+    for (int k = 0; k < NS; ++k) omega[k] += mech<R>().nu_net[i][k] * r;
   }
 }
 
