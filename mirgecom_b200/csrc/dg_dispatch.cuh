@@ -107,6 +107,22 @@ inline int prepare_kernel(Kern kern, size_t smem) {
   return MGC_OK;
 }
 
+// Grid of a persistent kernel: every CTA that fits on the device at once
+// (occupancy for this block size and shared memory times the SM count),
+// capped at the number of work tiles.
+template <class Kern>
+inline int persistent_grid(Kern kern, int threads, size_t smem, int64_t tiles, int* nblk) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess)
+    return MGC_E_CUDA;
+  int64_t nb = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
+  if (nb > tiles) nb = tiles;
+  *nblk = (int)(nb > 0 ? nb : 1);
+  return MGC_OK;
+}
+
 template <class R, int DIM, int ORDER, int NS, bool MIX>
 struct Launch {
   using C = Cfg<R, DIM, ORDER, NS, MIX>;
@@ -130,7 +146,10 @@ struct Launch {
     auto kern = k_surface<R, DIM, ORDER, NS, MIX, VISC>;
     int rc = prepare_kernel(kern, smem);
     if (rc) return rc;
-    const int nblk = (a.nelem + C::EPB_SURF - 1) / C::EPB_SURF;
+    const int ntiles = (a.nelem + C::EPB_SURF - 1) / C::EPB_SURF;
+    int nblk = 0;
+    rc = persistent_grid(kern, C::NT, smem, ntiles, &nblk);
+    if (rc) return rc;
     kern<<<nblk, C::NT, smem, s>>>(a, g);
     return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
   }

@@ -134,10 +134,10 @@ struct Cfg {
   // p, c, gamma (padded to 16 bytes); the surface kernel holds only the
   // contraction operands in shared memory
   static constexpr int FW = round_up(NC * DIM + 3, 4);
-  static constexpr int S_BUDGET = 74 * 1024;
+  static constexpr int S_BUDGET = (RB == 8 ? 100 : 74) * 1024;
   // resident blocks: float64 mixture state needs more registers per thread
   static constexpr int MINB_NODE = (RB == 8 && NS > 2) ? 3 : 4;
-  static constexpr int MINB_SURF = (RB == 8 && NS > 2) ? 1 : 2;
+  static constexpr int MINB_SURF = 2;
   static constexpr int S_PER_ELEM = NC * KB + GEO;
   static constexpr int EPB_S_RAW = (S_BUDGET / RB - R_MAT - 1024 / RB) / S_PER_ELEM;
   static constexpr int EPB_SURF = imax(4, imin(32, EPB_S_RAW >= 8 ? EPB_S_RAW / 8 * 8
@@ -959,47 +959,168 @@ __device__ __forceinline__ void load_record(const R* __restrict__ src, R (&rec)[
   }
 }
 
-// Exterior state and its total flux . n on a prescribed boundary face node
-// (interior gradients on both sides, mirgecom/boundary.py:141-146).  Kept
-// out of line: it runs on boundary faces only and would otherwise inflate the
-// register allocation of the interior path.
-template <class R, int DIM, int NS, bool MIX, bool VISC>
-__device__ __noinline__ void prescribed_exterior_flux(const DGArgs<R>& a, const GasParams& g,
-                                                      const R* qp, R t_ext, int64_t gm,
-                                                      int64_t EN, const R* n,
-                                                      NodeState<R, DIM, NS>& sp, R* fpn) {
-  constexpr int NC = DIM + 2 + NS;
-  make_state<R, DIM, NS>(qp, t_ext, g, sp);
-  R fe[NC][DIM];
-  inviscid_flux<R, DIM, NS>(sp, fe);
+// Record values [v0, v0 + GV) of one node into registers, in 16-byte loads;
+// chunks that start at or beyond *lim* (the end of the flux part of the
+// record) are skipped.
+template <class R, int GV>
+__device__ __forceinline__ void load_group(const R* __restrict__ src, int v0, int lim,
+                                           R (&v)[GV]) {
+  if constexpr (sizeof(R) == 4) {
 #pragma unroll
-  for (int c = 0; c < NC; ++c)
+    for (int i = 0; i < GV; i += 4) {
+      float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (v0 + i < lim) x = *reinterpret_cast<const float4*>(src + v0 + i);
+      v[i] = x.x;
+      v[i + 1] = x.y;
+      v[i + 2] = x.z;
+      v[i + 3] = x.w;
+    }
+  } else {
 #pragma unroll
-    for (int j = 0; j < DIM; ++j) fe[c][j] = -fe[c][j];
-  if (VISC) {
-    R gqp[NC][DIM], gtp[DIM];
-#pragma unroll
-    for (int c = 0; c < NC; ++c)
-#pragma unroll
-      for (int j = 0; j < DIM; ++j) gqp[c][j] = a.grad[((int64_t)c * DIM + j) * EN + gm];
-#pragma unroll
-    for (int j = 0; j < DIM; ++j) gtp[j] = a.grad[((int64_t)NC * DIM + j) * EN + gm];
-    R fv[NC][DIM];
-    viscous_flux<R, DIM, NS, MIX>(sp, gqp, gtp, fv);
-#pragma unroll
-    for (int c = 0; c < NC; ++c)
-#pragma unroll
-      for (int j = 0; j < DIM; ++j) fe[c][j] += fv[c][j];
-  }
-#pragma unroll
-  for (int c = 0; c < NC; ++c) {
-    R acc = R(0);
-#pragma unroll
-    for (int j = 0; j < DIM; ++j) acc += fe[c][j] * n[j];
-    fpn[c] = acc;
+    for (int i = 0; i < GV; i += 2) {
+      double2 x = make_double2(0.0, 0.0);
+      if (v0 + i < lim) x = *reinterpret_cast<const double2*>(src + v0 + i);
+      v[i] = x.x;
+      v[i + 1] = x.y;
+    }
   }
 }
 
+// One face node of the surface pass evaluated from full face states: HLL on
+// interior faces, prescribed and dummy boundaries, and pairings that fail the
+// index checks.  Follows mirgecom/inviscid.py:290-376 and viscous.py:431-544
+// (F* = central(F_V) - numflux(F_I)), boundary.py:141-146 (prescribed: the
+// exterior state with the interior gradients) and boundary.py:1027-1049
+// (dummy: the interior flux).  Writes S_c = fsc (F*_c - F0_c . n) for every
+// field c to bcol[c * cstride].  Out of line (arguments by value, no
+// address of a caller variable taken), so that its face states do not enter
+// the register allocation of the interior fast path.
+template <class R, int DIM, int ORDER, int NS, bool MIX, bool VISC>
+__device__ __noinline__ void surface_face_general(const DGArgs<R> a, const GasParams g,
+                                                  int64_t EN, int64_t gm, int64_t g0, int m,
+                                                  int cn, R n0, R n1, R n2, R fsc,
+                                                  const uint8_t* perm_s, R* bcol, int cstride) {
+  const R n[3] = {n0, n1, n2};
+  using C = Cfg<R, DIM, ORDER, NS, MIX>;
+  constexpr int NP = C::NP, NFP = C::NFP, NC = C::NC, FW = C::FW;
+  const int E = a.nelem;
+  R fr[FW], f0[FW];
+  load_record<R, FW>(a.fbuf + gm * FW, fr);
+  load_record<R, FW>(a.fbuf + g0 * FW, f0);
+  R qm[NC], qp[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) qm[c] = a.q[c * EN + gm];
+  NodeState<R, DIM, NS> sm, sp;
+  make_state_light<R, DIM, NS>(qm, fr[NC * DIM], fr[NC * DIM + 1], fr[NC * DIM + 2], sm);
+  R ftm[NC], f0n[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    R acc = R(0), acc0 = R(0);
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) {
+      acc += fr[c * DIM + j] * n[j];
+      acc0 += f0[c * DIM + j] * n[j];
+    }
+    ftm[c] = acc;
+    f0n[c] = acc0;
+  }
+  int mode = 0;   // 0 two-sided, 1 interior flux only (dummy / bad pairing)
+  R fpn[NC];
+  if (cn >= 0) {
+    const int en = cn >> 8, pr = cn & 255;
+    const int kn = (pr < a.nperm) ? perm_s[pr * NFP + m] : NP;
+    if (en >= E || kn >= NP) {
+      atomicOr(a.status, ST_BAD_INDEX);
+      mode = 1;
+    } else {
+      const int64_t gi = (int64_t)en * NP + kn;
+      load_record<R, FW>(a.fbuf + gi * FW, fr);     // reuse: neighbour record
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        qp[c] = a.q[c * EN + gi];
+        R acc = R(0);
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) acc += fr[c * DIM + j] * n[j];
+        fpn[c] = acc;
+      }
+      make_state_light<R, DIM, NS>(qp, fr[NC * DIM], fr[NC * DIM + 1], fr[NC * DIM + 2], sp);
+    }
+  } else {
+    const int bf = -(cn + 1);
+    const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
+    if (kind == BK_PRESCRIBED) {
+      const int64_t bstride = (int64_t)a.nbf * NFP;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) qp[c] = a.bext[c * bstride + (int64_t)bf * NFP + m];
+      make_state<R, DIM, NS>(qp, MIX ? a.bext[NC * bstride + (int64_t)bf * NFP + m] : R(0), g,
+                             sp);
+      R fe[NC][DIM];
+      inviscid_flux<R, DIM, NS>(sp, fe);
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) fe[c][j] = -fe[c][j];
+      if (VISC) {
+        R gqp[NC][DIM], gtp[DIM];
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+          for (int j = 0; j < DIM; ++j) gqp[c][j] = a.grad[((int64_t)c * DIM + j) * EN + gm];
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) gtp[j] = a.grad[((int64_t)NC * DIM + j) * EN + gm];
+        R fv[NC][DIM];
+        viscous_flux<R, DIM, NS, MIX>(sp, gqp, gtp, fv);
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+          for (int j = 0; j < DIM; ++j) fe[c][j] += fv[c][j];
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        R acc = R(0);
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) acc += fe[c][j] * n[j];
+        fpn[c] = acc;
+      }
+    } else {
+      if (kind < 0) atomicOr(a.status, ST_BAD_INDEX);
+      mode = 1;
+    }
+  }
+  if (mode == 1) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) bcol[c * cstride] = fsc * (ftm[c] - f0n[c]);
+  } else {
+    // F_V . n = F . n + F_I . n on each side
+    R fi[NC], fim[NC], fip[NC];
+    inviscid_num_flux<R, DIM, NS>(sm, sp, qm, qp, n, a.flux_kind, fi);
+    inviscid_flux_n<R, DIM, NS>(sm, n, fim);
+    inviscid_flux_n<R, DIM, NS>(sp, n, fip);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      R out = -fi[c];
+      if (VISC) out += ((ftm[c] + fim[c]) + (fpn[c] + fip[c])) / R(2);
+      bcol[c * cstride] = fsc * (out - f0n[c]);
+    }
+  }
+}
+
+// Surface and lift pass of the split divergence: a persistent kernel (one
+// grid of resident CTAs) that builds the [-W | LIFT] operand once per CTA and
+// then loops over element tiles:
+//   volume  G_r = sum_j (dr_r/dx_j)(F_j - F0_j) from the flux records, one
+//           (node, group of four fields) per work item
+//   faces   one (face node, field group) per work item.  On interior faces
+//           with the Rusanov or central flux the records already hold the
+//           total flux F = F_V - F_I on both sides, so
+//               F*_V - F*_I = (F^- + F^+) . n / 2 - lambda (q^- - q^+) / 2
+//           (lambda = max(|v| + c) for Rusanov, 0 for central): no face
+//           state is rebuilt.  Other faces take surface_face_general.
+//   lift    rhs = [-W | LIFT] [G ; S] on the tensor cores, one (n-tile,
+//           m-tile) per warp work item, plus the species sources.
+// F0 is the record of the element's node 0: subtracting an element-constant
+// flux from every volume and face value leaves the discrete divergence
+// unchanged and keeps the contraction operands small.
 template <class R, int DIM, int ORDER, int NS, bool MIX, bool VISC>
 __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
     k_surface(DGArgs<R> a, GasParams g) {
@@ -1008,6 +1129,10 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
   constexpr int NP = C::NP, NF = C::NF, NFP = C::NFP, NFN = C::NFN, NC = C::NC, FW = C::FW;
   constexpr int EPB = C::EPB_SURF, MP = C::MP, MT = C::MT, KB = C::KB, KR = C::KR;
   constexpr int KRR = C::KRR, NCOL = C::NCOL_S;
+  constexpr int CG = 4;                     // fields per work item
+  constexpr int NG = (NC + CG - 1) / CG;    // field groups
+  constexpr int GV = CG * DIM;              // record values per group
+  constexpr int LIM = NC * DIM;             // end of the flux part of a record
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* am = reinterpret_cast<R*>(smem_raw);                  // [NAC][MP][KB]
   R* bm = am + C::NAC * MP * KB;                           // [NCOL][KB]
@@ -1018,8 +1143,6 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
   uint8_t* perm_s = reinterpret_cast<uint8_t*>(fn_s + NFN);
 
   const int E = a.nelem;
-  const int e0 = blockIdx.x * EPB;
-  const int ne = imin(EPB, E - e0);
   const int64_t EN = (int64_t)E * NP;
   const bool sources = MIX && a.add_sources;
 
@@ -1036,169 +1159,144 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
     }
     put_a<R>(am, MP * KB, i, v);
   }
+  // padding rows/columns of B stay zero for the whole kernel
   for (int i = threadIdx.x; i < NCOL * KB; i += blockDim.x) bm[i] = R(0);
   for (int i = threadIdx.x; i < NFN; i += blockDim.x) fn_s[i] = c_face_nodes<DIM, ORDER>(i);
   for (int i = threadIdx.x; i < a.nperm * NFP; i += blockDim.x) perm_s[i] = a.perm[i];
-  load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
-  __syncthreads();
 
-  // volume terms: G_r = sum_j (dr_r/dx_j) F_j, shifted by the node-0 value
-  for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
-    const int e = idx / NP, k = idx % NP;
-    R f[FW], f0[FW];
-    load_record<R, FW>(a.fbuf + ((int64_t)e0 * NP + idx) * FW, f);
-    load_record<R, FW>(a.fbuf + ((int64_t)(e0 + e) * NP) * FW, f0);
-#pragma unroll
-    for (int c = 0; c < NC; ++c)
-#pragma unroll
-      for (int r = 0; r < DIM; ++r) {
-        R acc = R(0);
-#pragma unroll
-        for (int j = 0; j < DIM; ++j)
-          acc += rx_s[e * DIM * DIM + r * DIM + j] * (f[c * DIM + j] - f0[c * DIM + j]);
-        bm[(c * EPB + e) * KB + r * NP + k] = acc;
-      }
-  }
-
-  // numerical face fluxes from the records of both sides
-  for (int idx = threadIdx.x; idx < ne * NFN; idx += blockDim.x) {
-    const int e = idx / NFN, fm = idx % NFN, f = fm / NFP, m = fm % NFP;
-    const int k = fn_s[fm];
-    const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
-    const R fsc = fs_s[e * NF + f];
-    R n[DIM];
-#pragma unroll
-    for (int j = 0; j < DIM; ++j) n[j] = nrm_s[(e * NF + f) * DIM + j];
-    const int64_t gm = (int64_t)(e0 + e) * NP + k;
-    R fr[FW], f0[FW];
-    load_record<R, FW>(a.fbuf + gm * FW, fr);
-    load_record<R, FW>(a.fbuf + ((int64_t)(e0 + e) * NP) * FW, f0);
-    R qm[NC], qp[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) qm[c] = a.q[c * EN + gm];
-    NodeState<R, DIM, NS> sm, sp;
-    make_state_light<R, DIM, NS>(qm, fr[NC * DIM], fr[NC * DIM + 1], fr[NC * DIM + 2], sm);
-    R ftm[NC], f0n[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      R acc = R(0), acc0 = R(0);
-#pragma unroll
-      for (int j = 0; j < DIM; ++j) {
-        acc += fr[c * DIM + j] * n[j];
-        acc0 += f0[c * DIM + j] * n[j];
-      }
-      ftm[c] = acc;
-      f0n[c] = acc0;
-    }
-    int mode = 0;   // 0 interior, 1 dummy (interior only), 2 prescribed exterior
-    R fpn[NC];
-    if (cn >= 0) {
-      const int en = cn >> 8, pr = cn & 255;
-      const int kn = (pr < a.nperm) ? perm_s[pr * NFP + m] : NP;
-      if (en >= E || kn >= NP) {
-        atomicOr(a.status, ST_BAD_INDEX);
-        mode = 1;
-      } else {
-        const int64_t gi = (int64_t)en * NP + kn;
-        load_record<R, FW>(a.fbuf + gi * FW, fr);     // reuse: neighbour record
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          qp[c] = a.q[c * EN + gi];
-          R acc = R(0);
-#pragma unroll
-          for (int j = 0; j < DIM; ++j) acc += fr[c * DIM + j] * n[j];
-          fpn[c] = acc;
-        }
-        make_state_light<R, DIM, NS>(qp, fr[NC * DIM], fr[NC * DIM + 1], fr[NC * DIM + 2], sp);
-      }
-    } else {
-      const int bf = -(cn + 1);
-      const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
-      if (kind == BK_PRESCRIBED) {
-        mode = 2;
-        const int64_t bstride = (int64_t)a.nbf * NFP;
-#pragma unroll
-        for (int c = 0; c < NC; ++c) qp[c] = a.bext[c * bstride + (int64_t)bf * NFP + m];
-        prescribed_exterior_flux<R, DIM, NS, MIX, VISC>(
-            a, g, qp, MIX ? a.bext[NC * bstride + (int64_t)bf * NFP + m] : R(0), gm, EN, n, sp,
-            fpn);
-      } else {
-        if (kind < 0) atomicOr(a.status, ST_BAD_INDEX);
-        mode = 1;
-      }
-    }
-    R out[NC];
-    if (mode == 1) {
-      // DummyBoundary: F_V(q-).n - F_I(q-).n  (boundary.py:1027-1049)
-#pragma unroll
-      for (int c = 0; c < NC; ++c) out[c] = ftm[c];
-    } else {
-      // F* = central(F_V) - numflux(F_I);  F_V.n = F.n + F_I.n on each side
-      R fi[NC], fim[NC], fip[NC];
-      inviscid_num_flux<R, DIM, NS>(sm, sp, qm, qp, n, a.flux_kind, fi);
-      inviscid_flux_n<R, DIM, NS>(sm, n, fim);
-      inviscid_flux_n<R, DIM, NS>(sp, n, fip);
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        out[c] = -fi[c];
-        if (VISC) out[c] += ((ftm[c] + fim[c]) + (fpn[c] + fip[c])) / R(2);
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < NC; ++c) bm[(c * EPB + e) * KB + DIM * NP + fm] = fsc * (out[c] - f0n[c]);
-  }
-  __syncthreads();
-
-  // rhs = [-W | LIFT] [G ; S] on the tensor cores (+ sources)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gq = lane >> 2, tq = lane & 3;
+  const int nwarps = blockDim.x >> 5;
   constexpr int NACC = C::TF32 ? 4 : 2;
+  const int ntiles = (E + EPB - 1) / EPB;
   bool bad = false;
-  for (int nt = warp; nt < NCOL / 8; nt += blockDim.x >> 5) {
-    R d[MT][NACC];
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int e0 = tile * EPB;
+    const int ne = imin(EPB, E - e0);
+    // (its first barrier also orders the previous tile's contraction reads
+    // of bm before this tile's writes)
+    load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
+    __syncthreads();
+
+    // volume terms
+    for (int it = threadIdx.x; it < ne * NP * NG; it += blockDim.x) {
+      const int grp = it % NG, node = it / NG;
+      const int e = node / NP, k = node % NP;
+      R fv[GV], f0v[GV];
+      load_group<R, GV>(a.fbuf + ((int64_t)e0 * NP + node) * FW, grp * GV, LIM, fv);
+      load_group<R, GV>(a.fbuf + ((int64_t)(e0 + e) * NP) * FW, grp * GV, LIM, f0v);
+      const R* rxe = rx_s + e * DIM * DIM;
 #pragma unroll
-    for (int t = 0; t < MT; ++t)
+      for (int cc = 0; cc < CG; ++cc) {
+        const int c = grp * CG + cc;
+        if (c >= NC) break;
 #pragma unroll
-      for (int v = 0; v < NACC; ++v) d[t][v] = R(0);
-    const R* bcol = bm + (nt * 8 + gq) * KB + tq;
-    if constexpr (!C::TF32) {
-#pragma unroll 5
-      for (int ks = 0; ks < KRR / 4; ++ks) {
-        const double b = bcol[ks * 4];
+        for (int r = 0; r < DIM; ++r) {
+          R acc = R(0);
 #pragma unroll
-        for (int t = 0; t < MT; ++t) dmma884(d[t], am[(t * 8 + gq) * KB + ks * 4 + tq], b);
+          for (int j = 0; j < DIM; ++j)
+            acc += rxe[r * DIM + j] * (fv[cc * DIM + j] - f0v[cc * DIM + j]);
+          bm[(c * EPB + e) * KB + r * NP + k] = acc;
+        }
       }
-    } else {
-#pragma unroll 2
-      for (int ks = 0; ks < KRR / 8; ++ks) {
-        const float b0 = bcol[ks * 8], b1 = bcol[ks * 8 + 4];
+    }
+
+    // face terms
+    for (int it = threadIdx.x; it < ne * NFN * NG; it += blockDim.x) {
+      const int grp = it % NG, fnode = it / NG;
+      const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
+      const int k = fn_s[fm];
+      const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
+      const R fsc = fs_s[e * NF + f];
+      R n[DIM];
 #pragma unroll
-        for (int t = 0; t < MT; ++t) {
+      for (int j = 0; j < DIM; ++j) n[j] = nrm_s[(e * NF + f) * DIM + j];
+      const int64_t gm = (int64_t)(e0 + e) * NP + k, g0 = (int64_t)(e0 + e) * NP;
+      R* bcol = bm + e * KB + DIM * NP + fm;
+      int64_t gi = -1;
+      if (cn >= 0 && a.flux_kind != FLUX_HLL) {
+        const int en = cn >> 8, pr = cn & 255;
+        const int kn = (pr < a.nperm) ? perm_s[pr * NFP + m] : NP;
+        if (en < E && kn < NP) gi = (int64_t)en * NP + kn;
+      }
+      if (gi >= 0) {
+        R lam = R(0);
+        if (a.flux_kind == FLUX_RUSANOV) {
+          const R irm = R(1) / a.q[gm], irp = R(1) / a.q[gi];
+          R vm2 = R(0), vp2 = R(0);
+#pragma unroll
+          for (int j = 0; j < DIM; ++j) {
+            const R vm = a.q[(2 + j) * EN + gm] * irm, vp = a.q[(2 + j) * EN + gi] * irp;
+            vm2 += vm * vm;
+            vp2 += vp * vp;
+          }
+          lam = fmax(sqrt(vm2) + a.fbuf[gm * FW + LIM + 1], sqrt(vp2) + a.fbuf[gi * FW + LIM + 1]);
+        }
+        R fmv[GV], fpv[GV], f0v[GV];
+        load_group<R, GV>(a.fbuf + gm * FW, grp * GV, LIM, fmv);
+        load_group<R, GV>(a.fbuf + gi * FW, grp * GV, LIM, fpv);
+        load_group<R, GV>(a.fbuf + g0 * FW, grp * GV, LIM, f0v);
+#pragma unroll
+        for (int cc = 0; cc < CG; ++cc) {
+          const int c = grp * CG + cc;
+          if (c >= NC) break;
+          R sm_ = R(0), sp_ = R(0), s0 = R(0);
+#pragma unroll
+          for (int j = 0; j < DIM; ++j) {
+            sm_ += fmv[cc * DIM + j] * n[j];
+            sp_ += fpv[cc * DIM + j] * n[j];
+            s0 += f0v[cc * DIM + j] * n[j];
+          }
+          const R dq = a.q[c * EN + gm] - a.q[c * EN + gi];
+          const R out = (sm_ + sp_) / R(2) - lam * dq / R(2);
+          bcol[c * EPB * KB] = fsc * (out - s0);
+        }
+      } else if (grp == 0) {
+        surface_face_general<R, DIM, ORDER, NS, MIX, VISC>(
+            a, g, EN, gm, g0, m, cn, n[0], n[1], DIM > 2 ? n[DIM - 1] : R(0), fsc, perm_s,
+            bcol, EPB * KB);
+      }
+    }
+    __syncthreads();
+
+    // rhs = [-W | LIFT] [G ; S] on the tensor cores (+ sources)
+    for (int w = warp; w < (NCOL / 8) * MT; w += nwarps) {
+      const int nt = w / MT, t = w % MT;
+      R d[NACC];
+#pragma unroll
+      for (int v = 0; v < NACC; ++v) d[v] = R(0);
+      const R* bcol = bm + (nt * 8 + gq) * KB + tq;
+      if constexpr (!C::TF32) {
+#pragma unroll 5
+        for (int ks = 0; ks < KRR / 4; ++ks)
+          dmma884(d, am[(t * 8 + gq) * KB + ks * 4 + tq], bcol[ks * 4]);
+      } else {
+#pragma unroll 2
+        for (int ks = 0; ks < KRR / 8; ++ks) {
+          const float b0 = bcol[ks * 8], b1 = bcol[ks * 8 + 4];
           uint32_t ah[4], alo[4];
           load_a_tf32(ah, am, KB, t * 16, ks * 8, gq, tq);
           load_a_tf32(alo, am + MP * KB, KB, t * 16, ks * 8, gq, tq);
-          mma_tf32x3(d[t], ah, alo, b0, b1);
+          mma_tf32x3(d, ah, alo, b0, b1);
         }
       }
-    }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int col = nt * 8 + 2 * tq + h;
-      const int c = col / EPB, e = col % EPB;
-      if (c >= NC || e >= ne) continue;
-      R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
-#pragma unroll
-      for (int t = 0; t < MT; ++t)
+      for (int h = 0; h < 2; ++h) {
+        const int col = nt * 8 + 2 * tq + h;
+        const int c = col / EPB, e = col % EPB;
+        if (c >= NC || e >= ne) continue;
+        R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
 #pragma unroll
         for (int half = 0; half < NACC / 2; ++half) {
           const int i = t * Tile<R>::MROW + gq + 8 * half;
           if (i >= NP) continue;
-          R v = d[t][2 * half + h];
+          R v = d[2 * half + h];
           if (sources && c >= 2 + DIM)
             v += a.srcbuf[(int64_t)(c - 2 - DIM) * EN + (int64_t)(e0 + e) * NP + i];
           outp[i] = v;
           bad |= !(v == v);
         }
+      }
     }
   }
   if (bad) atomicOr(a.status, ST_NAN);
