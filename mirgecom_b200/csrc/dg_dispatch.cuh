@@ -131,7 +131,10 @@ struct Launch {
     auto kern = k_grad<R, DIM, ORDER, NS, MIX>;
     int rc = prepare_kernel(kern, smem);
     if (rc) return rc;
-    const int nblk = (a.nelem + C::EPB_GRAD - 1) / C::EPB_GRAD;
+    const int ntiles = (a.nelem + C::EPB_GRAD - 1) / C::EPB_GRAD;
+    int nblk = 0;
+    rc = persistent_grid(kern, C::NT, smem, ntiles, &nblk);
+    if (rc) return rc;
     kern<<<nblk, C::NT, smem, s>>>(a, g);
     return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
   }

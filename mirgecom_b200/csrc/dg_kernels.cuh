@@ -112,7 +112,7 @@ struct Cfg {
   static constexpr int KS = T::stride(NF * NFPK);
   static constexpr int KL = T::stride(NFPK);
   static constexpr int G_MAT = NAC * (DIM * MP * KU + NF * MP * KL);
-  static constexpr int G_PER_ELEM = NU * (KU + KS) + GEO;
+  static constexpr int G_PER_ELEM = NU * (KU + KS + 1) + GEO;
   static constexpr int EPB_G_RAW = (SMEM_BUDGET / RB - G_MAT - 1024 / RB) / G_PER_ELEM;
   static constexpr int EPB_GRAD = imax(8, imin(32, EPB_G_RAW / 8 * 8));
   static constexpr int NCOL_G = round_up(NU * EPB_GRAD, 8);
@@ -148,9 +148,10 @@ struct Cfg {
            64;
   }
 
+  static constexpr int MINB_GRAD = 2;
   static size_t smem_grad(int nperm) {
-    return (size_t)(G_MAT + NCOL_G * (KU + KS) + EPB_GRAD * GEO) * RB + NFN * 4 +
-           (size_t)nperm * NFP + 64;
+    return (size_t)(G_MAT + NCOL_G * (KU + KS) + EPB_GRAD * GEO + NU * EPB_GRAD) * RB +
+           NFN * 4 + (size_t)nperm * NFP + 64;
   }
   static size_t smem_rhs(int nperm) {
     return (size_t)(R_MAT + NCOL_R * KB +
@@ -353,8 +354,18 @@ __global__ void __launch_bounds__(256) k_mixture_state_mixed(
 
 // {{{ gradient kernel
 
+// Gradient pass (grad_cv_operator + grad_t_operator): a persistent kernel
+// that builds W_r and LIFT_f once per CTA and loops over element tiles:
+//   phase 1  U = u - u0 per node (u0 the element's node-0 value; the discrete
+//            gradient of a constant vanishes, so the shift keeps large means
+//            out of the contraction and changes nothing in exact arithmetic)
+//   phase 2  S = fscale (u* - u0) per face node and group of four fields,
+//            u* the BR1 central value, the prescribed exterior value, or the
+//            interior value (dummy boundary)
+//   phase 3  du_r = W_r U, L_f = LIFT_f S on the tensor cores per (n-tile,
+//            m-tile), grad_j = sum_f n_fj L_f - sum_r (dr_r/dx_j) du_r
 template <class R, int DIM, int ORDER, int NS, bool MIX>
-__global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
+__global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
     k_grad(DGArgs<R> a, GasParams g) {
   using C = Cfg<R, DIM, ORDER, NS, MIX>;
   using S = Simplex<DIM, ORDER>;
@@ -363,6 +374,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
   constexpr int KU = C::KU, KS = C::KS, KL = C::KL, NFPK = C::NFPK, NCOL = C::NCOL_G;
   constexpr int KUR = C::KUR;
   constexpr int AWN = DIM * MP * KU, ALN = NF * MP * KL;
+  constexpr int CG = 4, NGU = (NU + CG - 1) / CG;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* aw = reinterpret_cast<R*>(smem_raw);                  // [NAC][DIM][MP][KU]
   R* al = aw + NAC * AWN;                                  // [NAC][NF][MP][KL]
@@ -371,12 +383,11 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
   R* rx_s = bs + NCOL * KS;                                // [EPB][DIM][DIM]
   R* nrm_s = rx_s + EPB * DIM * DIM;                       // [EPB][NF][DIM]
   R* fs_s = nrm_s + EPB * NF * DIM;                        // [EPB][NF]
-  int* fn_s = reinterpret_cast<int*>(fs_s + EPB * NF);     // [NF*NFP]
+  R* u0_s = fs_s + EPB * NF;                               // [NU][EPB]
+  int* fn_s = reinterpret_cast<int*>(u0_s + NU * EPB);     // [NF*NFP]
   uint8_t* perm_s = reinterpret_cast<uint8_t*>(fn_s + NFN);
 
   const int E = a.nelem;
-  const int e0 = blockIdx.x * EPB;
-  const int ne = imin(EPB, E - e0);
   const int64_t EN = (int64_t)E * NP;
 
   // reference operators (zero padded; hi/lo tf32 split on the mixed path)
@@ -389,168 +400,168 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
     put_a<R>(al, ALN, i,
              (row < NP && m < NFP) ? c_ref64[S::OFF_LIFT + row * NFN + f * NFP + m] : 0.0);
   }
+  // padding rows/columns of the B operands stay zero for the whole kernel
   for (int i = threadIdx.x; i < NCOL * (KU + KS); i += blockDim.x) bu[i] = R(0);
   for (int i = threadIdx.x; i < NFN; i += blockDim.x) fn_s[i] = c_face_nodes<DIM, ORDER>(i);
   for (int i = threadIdx.x; i < a.nperm * NFP; i += blockDim.x) perm_s[i] = a.perm[i];
-  load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);   // syncs once
-  __syncthreads();
 
-  // phase 1: conserved fields and temperature of the tile into U
-  for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
-    const int e = idx / NP, k = idx % NP;
-    R qq[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      qq[c] = a.q[c * EN + (int64_t)e0 * NP + idx];
-      bu[(c * EPB + e) * KU + k] = qq[c];
-    }
-    bu[(NC * EPB + e) * KU + k] =
-        MIX ? a.t_op[(int64_t)e0 * NP + idx] : node_temperature<R, DIM, NS>(qq, R(0), g);
-  }
-  __syncthreads();
-
-  // phase 3: face values  fscale * u*   (u* = central average or boundary value)
-  for (int idx = threadIdx.x; idx < ne * NFN; idx += blockDim.x) {
-    const int e = idx / NFN, fm = idx % NFN, f = fm / NFP, m = fm % NFP;
-    const int k = fn_s[fm];
-    const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
-    const R fsc = fs_s[e * NF + f];
-    R up[NU];
-    bool central = true;
-    if (cn >= 0) {
-      const int en = cn >> 8, pr = cn & 255;
-      const int kn = (pr < a.nperm) ? perm_s[pr * NFP + m] : NP;
-      if (en >= E || kn >= NP) {
-        atomicOr(a.status, ST_BAD_INDEX);
-#pragma unroll
-        for (int c = 0; c < NU; ++c) up[c] = bu[(c * EPB + e) * KU + k];
-      } else {
-        const int64_t gi = (int64_t)en * NP + kn;
-#pragma unroll
-        for (int c = 0; c < NC; ++c) up[c] = a.q[c * EN + gi];
-        up[NC] = MIX ? a.t_op[gi] : node_temperature<R, DIM, NS>(up, R(0), g);
-      }
-    } else {
-      const int bf = -(cn + 1);
-      const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
-      if (kind == BK_PRESCRIBED) {
-        const int64_t bstride = (int64_t)a.nbf * NFP;
-#pragma unroll
-        for (int c = 0; c < NC; ++c) up[c] = a.bext[c * bstride + (int64_t)bf * NFP + m];
-        up[NC] = MIX ? a.bext[NC * bstride + (int64_t)bf * NFP + m]
-                     : node_temperature<R, DIM, NS>(up, R(0), g);
-        central = false;   // the gradient flux sends the exterior value
-      } else {
-        if (kind < 0) atomicOr(a.status, ST_BAD_INDEX);
-#pragma unroll
-        for (int c = 0; c < NU; ++c) up[c] = bu[(c * EPB + e) * KU + k];
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < NU; ++c) {
-      const R um = bu[(c * EPB + e) * KU + k];
-      const R ustar = central ? (up[c] + um) / R(2) : up[c];
-      // element-constant shift (node 0 value): the discrete gradient of a
-      // constant vanishes, so subtracting it changes nothing in exact
-      // arithmetic and keeps large means out of the contraction
-      bs[(c * EPB + e) * KS + f * NFPK + m] = fsc * (ustar - bu[(c * EPB + e) * KU]);
-    }
-  }
-  __syncthreads();
-  for (int p = threadIdx.x; p < NU * ne; p += blockDim.x) {
-    const int c = p / ne, e = p % ne;
-    R* row = bu + (c * EPB + e) * KU;
-    const R u0 = row[0];
-#pragma unroll 4
-    for (int k = 0; k < NP; ++k) row[k] -= u0;
-  }
-  __syncthreads();
-
-  // phase 4: per 8-column tile, du_r = W_r U and L_f = LIFT_f S on the tensor
-  // cores, then grad_j = sum_f n_fj L_f - sum_r rx_rj du_r
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gq = lane >> 2, tq = lane & 3;
+  const int nwarps = blockDim.x >> 5;
   constexpr int NACC = C::TF32 ? 4 : 2;     // accumulator entries per lane per m-tile
-  for (int nt = warp; nt < NCOL / 8; nt += blockDim.x >> 5) {
-    R du[DIM][MT][NACC], lf[NF][MT][NACC];
+  const int ntiles = (E + EPB - 1) / EPB;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int e0 = tile * EPB;
+    const int ne = imin(EPB, E - e0);
+    // (its first barrier also orders the previous tile's contraction reads
+    // of bu / bs before this tile's writes)
+    load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
+
+    // phase 1: shifted conserved fields and temperature
+    for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
+      const int e = idx / NP, k = idx % NP;
+      const int64_t gn = (int64_t)e0 * NP + idx, g0 = (int64_t)(e0 + e) * NP;
+      R qq[NC], q0[NC];
 #pragma unroll
-    for (int r = 0; r < DIM; ++r)
+      for (int c = 0; c < NC; ++c) {
+        qq[c] = a.q[c * EN + gn];
+        q0[c] = a.q[c * EN + g0];
+      }
+      const R t = MIX ? a.t_op[gn] : node_temperature<R, DIM, NS>(qq, R(0), g);
+      const R t0 = MIX ? a.t_op[g0] : node_temperature<R, DIM, NS>(q0, R(0), g);
 #pragma unroll
-      for (int t = 0; t < MT; ++t)
+      for (int c = 0; c < NC; ++c) bu[(c * EPB + e) * KU + k] = qq[c] - q0[c];
+      bu[(NC * EPB + e) * KU + k] = t - t0;
+      if (k == 0) {
 #pragma unroll
-        for (int v = 0; v < NACC; ++v) du[r][t][v] = R(0);
+        for (int c = 0; c < NC; ++c) u0_s[c * EPB + e] = q0[c];
+        u0_s[NC * EPB + e] = t0;
+      }
+    }
+    __syncthreads();
+
+    // phase 2: face values  fscale * (u* - u0)
+    for (int it = threadIdx.x; it < ne * NFN * NGU; it += blockDim.x) {
+      const int grp = it % NGU, fnode = it / NGU;
+      const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
+      const int k = fn_s[fm];
+      const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
+      const R fsc = fs_s[e * NF + f];
+      // 0: two-sided average with node gi; 1: prescribed exterior; 2: interior value
+      int mode = 2;
+      int64_t gi = 0;
+      int bf = 0;
+      if (cn >= 0) {
+        const int en = cn >> 8, pr = cn & 255;
+        const int kn = (pr < a.nperm) ? perm_s[pr * NFP + m] : NP;
+        if (en >= E || kn >= NP) {
+          if (grp == 0) atomicOr(a.status, ST_BAD_INDEX);
+        } else {
+          gi = (int64_t)en * NP + kn;
+          mode = 0;
+        }
+      } else {
+        bf = -(cn + 1);
+        const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
+        if (kind == BK_PRESCRIBED) {
+          mode = 1;
+        } else if (kind < 0 && grp == 0) {
+          atomicOr(a.status, ST_BAD_INDEX);
+        }
+      }
+      const int64_t bstride = (int64_t)a.nbf * NFP, bo = (int64_t)bf * NFP + m;
+      // exterior temperature (only the group holding field NC needs it)
+      R tp = R(0);
+      if (grp == NC / CG && mode != 2) {
+        if (MIX) {
+          tp = (mode == 0) ? a.t_op[gi] : a.bext[NC * bstride + bo];
+        } else {
+          R up[NC];
 #pragma unroll
-    for (int f = 0; f < NF; ++f)
-#pragma unroll
-      for (int t = 0; t < MT; ++t)
-#pragma unroll
-        for (int v = 0; v < NACC; ++v) lf[f][t][v] = R(0);
-    const R* bcol = bu + (nt * 8 + gq) * KU + tq;
-    const R* scol = bs + (nt * 8 + gq) * KS + tq;
-    if constexpr (!C::TF32) {
-#pragma unroll
-      for (int ks = 0; ks < KUR / 4; ++ks) {
-        const double b = bcol[ks * 4];
-#pragma unroll
-        for (int r = 0; r < DIM; ++r)
-#pragma unroll
-          for (int t = 0; t < MT; ++t)
-            dmma884(du[r][t], aw[(r * MP + t * 8 + gq) * KU + ks * 4 + tq], b);
+          for (int c = 0; c < NC; ++c) up[c] = (mode == 0) ? a.q[c * EN + gi] : a.bext[c * bstride + bo];
+          tp = node_temperature<R, DIM, NS>(up, R(0), g);
+        }
       }
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
-#pragma unroll
-        for (int ks = 0; ks < NFPK / 4; ++ks) {
-          const double b = scol[f * NFPK + ks * 4];
-#pragma unroll
-          for (int t = 0; t < MT; ++t)
-            dmma884(lf[f][t], al[(f * MP + t * 8 + gq) * KL + ks * 4 + tq], b);
+      for (int cc = 0; cc < CG; ++cc) {
+        const int c = grp * CG + cc;
+        if (c >= NU) break;
+        const R um = bu[(c * EPB + e) * KU + k];           // u- - u0
+        const R u0 = u0_s[c * EPB + e];
+        R v = um;
+        if (mode != 2) {
+          const R up = (c == NC) ? tp : (mode == 0 ? a.q[c * EN + gi] : a.bext[c * bstride + bo]);
+          v = (mode == 0) ? ((up - u0) + um) / R(2) : up - u0;
         }
-    } else {
+        bs[(c * EPB + e) * KS + f * NFPK + m] = fsc * v;
+      }
+    }
+    __syncthreads();
+
+    // phase 3: contraction and metric combination
+    for (int w = warp; w < (NCOL / 8) * MT; w += nwarps) {
+      const int nt = w / MT, t = w % MT;
+      R du[DIM][NACC], lf[NF][NACC];
 #pragma unroll
-      for (int ks = 0; ks < KUR / 8; ++ks) {
-        const float b0 = bcol[ks * 8], b1 = bcol[ks * 8 + 4];
+      for (int v = 0; v < NACC; ++v) {
 #pragma unroll
-        for (int r = 0; r < DIM; ++r)
+        for (int r = 0; r < DIM; ++r) du[r][v] = R(0);
 #pragma unroll
-          for (int t = 0; t < MT; ++t) {
+        for (int f = 0; f < NF; ++f) lf[f][v] = R(0);
+      }
+      const R* bcol = bu + (nt * 8 + gq) * KU + tq;
+      const R* scol = bs + (nt * 8 + gq) * KS + tq;
+      if constexpr (!C::TF32) {
+#pragma unroll
+        for (int ks = 0; ks < KUR / 4; ++ks) {
+          const double b = bcol[ks * 4];
+#pragma unroll
+          for (int r = 0; r < DIM; ++r)
+            dmma884(du[r], aw[(r * MP + t * 8 + gq) * KU + ks * 4 + tq], b);
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+          for (int ks = 0; ks < NFPK / 4; ++ks)
+            dmma884(lf[f], al[(f * MP + t * 8 + gq) * KL + ks * 4 + tq], scol[f * NFPK + ks * 4]);
+      } else {
+#pragma unroll
+        for (int ks = 0; ks < KUR / 8; ++ks) {
+          const float b0 = bcol[ks * 8], b1 = bcol[ks * 8 + 4];
+#pragma unroll
+          for (int r = 0; r < DIM; ++r) {
             uint32_t ah[4], alo[4];
             load_a_tf32(ah, aw + r * MP * KU, KU, t * 16, ks * 8, gq, tq);
             load_a_tf32(alo, aw + AWN + r * MP * KU, KU, t * 16, ks * 8, gq, tq);
-            mma_tf32x3(du[r][t], ah, alo, b0, b1);
+            mma_tf32x3(du[r], ah, alo, b0, b1);
           }
-      }
+        }
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
+        for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int ks = 0; ks < NFPK / 8; ++ks) {
-          const float b0 = scol[f * NFPK + ks * 8], b1 = scol[f * NFPK + ks * 8 + 4];
-#pragma unroll
-          for (int t = 0; t < MT; ++t) {
+          for (int ks = 0; ks < NFPK / 8; ++ks) {
+            const float b0 = scol[f * NFPK + ks * 8], b1 = scol[f * NFPK + ks * 8 + 4];
             uint32_t ah[4], alo[4];
             load_a_tf32(ah, al + f * MP * KL, KL, t * 16, ks * 8, gq, tq);
             load_a_tf32(alo, al + ALN + f * MP * KL, KL, t * 16, ks * 8, gq, tq);
-            mma_tf32x3(lf[f][t], ah, alo, b0, b1);
+            mma_tf32x3(lf[f], ah, alo, b0, b1);
           }
-        }
-    }
+      }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int col = nt * 8 + 2 * tq + h;
-      const int c = col / EPB, e = col % EPB;
-      if (c >= NU || e >= ne) continue;
-      R rxe[DIM][DIM], nre[NF][DIM];
+      for (int h = 0; h < 2; ++h) {
+        const int col = nt * 8 + 2 * tq + h;
+        const int c = col / EPB, e = col % EPB;
+        if (c >= NU || e >= ne) continue;
+        R rxe[DIM][DIM], nre[NF][DIM];
 #pragma unroll
-      for (int r = 0; r < DIM; ++r)
+        for (int r = 0; r < DIM; ++r)
 #pragma unroll
-        for (int j = 0; j < DIM; ++j) rxe[r][j] = rx_s[e * DIM * DIM + r * DIM + j];
+          for (int j = 0; j < DIM; ++j) rxe[r][j] = rx_s[e * DIM * DIM + r * DIM + j];
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
+        for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int j = 0; j < DIM; ++j) nre[f][j] = nrm_s[(e * NF + f) * DIM + j];
-      R* outp = a.out + ((int64_t)c * DIM) * EN + (int64_t)(e0 + e) * NP;
-#pragma unroll
-      for (int t = 0; t < MT; ++t)
+          for (int j = 0; j < DIM; ++j) nre[f][j] = nrm_s[(e * NF + f) * DIM + j];
+        R* outp = a.out + ((int64_t)c * DIM) * EN + (int64_t)(e0 + e) * NP;
 #pragma unroll
         for (int half = 0; half < NACC / 2; ++half) {
           const int i = t * Tile<R>::MROW + gq + 8 * half;
@@ -560,12 +571,13 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
           for (int j = 0; j < DIM; ++j) {
             R gsum = R(0);
 #pragma unroll
-            for (int f = 0; f < NF; ++f) gsum += nre[f][j] * lf[f][t][v];
+            for (int f = 0; f < NF; ++f) gsum += nre[f][j] * lf[f][v];
 #pragma unroll
-            for (int r = 0; r < DIM; ++r) gsum -= rxe[r][j] * du[r][t][v];
+            for (int r = 0; r < DIM; ++r) gsum -= rxe[r][j] * du[r][v];
             outp[(int64_t)j * EN + i] = gsum;
           }
         }
+      }
     }
   }
 }
