@@ -175,14 +175,18 @@ int mgc_ns_rhs_f32(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
                    const float* bext, int flux_kind, int add_sources, float* rhs,
                    int32_t* status, void* stream);
 
-/* Mixture temperature, mixed form: float32 Newton started from t_guess (the
- * learned guess; NULL to start from t_seed) and stopped once the update is
- * below 1e-5 of T, then a float64 residual check |e - e(T)| / (c_v T) <=
- * rtol that accepts the result and applies the float64 residual as a last
- * Newton step (remaining error of order rtol^2); a rejected result is
- * recomputed from the plain guess t_seed.  iters (nullable) receives the
- * float32 iteration count per node (+1000 when the fallback ran); nodes
- * failing both set MGC_ST_NEWTON_MISS. */
+/* Mixture temperature, mixed form (extends mirgecom/thermochemistry.py:126-167,
+ * which runs a fixed number of float64 iterations).  Float32 Newton from
+ * t_guess (the learned guess; NULL to start from t_seed), stopped once the
+ * predicted remaining error k dT^2 (k = max |c_v'| / (2 c_v) of the
+ * mechanism, quadratic convergence) is small enough for the last step; then
+ * the float64 residual correction corr = (e - e(T)) / c_v(T) is applied when
+ * its own predicted remainder k corr^2 is at most rtol |T| -- the relative
+ * temperature-update tolerance the reference drivers check, e.g. 1e-8 in
+ * mirgecom examples/autoignition.py:526-530.  A rejected result is recomputed
+ * from the plain guess t_seed.  iters (nullable) receives the float32
+ * iteration count per node (+1000 when the fallback ran); nodes failing both
+ * set MGC_ST_NEWTON_MISS. */
 int mgc_mixture_temperature_f32(int dim, const mgc_gas_t* gas, int64_t nnodes,
                                 const float* q, const float* t_seed, const float* t_guess,
                                 float* t_out, int32_t* iters, int maxit, float rtol,
@@ -232,6 +236,16 @@ typedef struct {
 
 int mgc_mlp_nparams(void);
 int mgc_mlp_refresh(const mgc_mlp_t* w, void* stream);
+
+/* Mixed-form mixture temperature with the learned guess computed in the same
+ * kernel (no counterpart in the reference, which has no learned guess): per
+ * node the network's guess, then the solve of mgc_mixture_temperature_f32
+ * with t_seed as the fallback.  Same arguments and status as that call plus
+ * the network w; requires mgc_set_mechanism. */
+int mgc_mixture_temperature_learned_f32(int dim, const mgc_gas_t* gas, int64_t nnodes,
+                                        const float* q, const float* t_seed,
+                                        const mgc_mlp_t* w, float* t_out, int32_t* iters,
+                                        int maxit, float rtol, int32_t* status, void* stream);
 
 /* Guess T for every node of a float32 state q [Nc][n] (nspecies == 7). */
 int mgc_mlp_infer(int dim, int nspecies, int64_t n, const float* q, const mgc_mlp_t* w,

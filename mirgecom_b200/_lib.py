@@ -92,6 +92,8 @@ _SIGNATURES = {
     "mgc_ns_rhs_f32": ([_P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P], C.c_int),
     "mgc_mixture_temperature_f32": (
         [C.c_int, _P, C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_float, _P, _P], C.c_int),
+    "mgc_mixture_temperature_learned_f32": (
+        [C.c_int, _P, C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_float, _P, _P], C.c_int),
     "mgc_rk4_stage_mixed": ([C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_double, _P], C.c_int),
     "mgc_rhs_split_workspace_bytes": ([_P, _P, C.c_int], C.c_size_t),
     "mgc_rhs_split": ([C.c_int, _P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P,

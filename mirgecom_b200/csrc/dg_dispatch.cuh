@@ -36,6 +36,22 @@ inline Mechanism expand_mechanism(const mgc_mechanism_t& m) {
       e[5] = a[6];
     }
   }
+  // Newton convergence constant: max over species and T in [200, 6000] K of
+  // |c_v'| / (2 c_v), c_v/R = a0 - 1 + a1 T + ... + a4 T^4 (1 K steps)
+  double kmax = 0.0;
+  for (int s = 0; s < m.nspecies && s < MGC_MAX_SPECIES; ++s) {
+    for (int ti = 200; ti <= 6000; ++ti) {
+      const double t = ti;
+      const double* a = (t > m.t_mid[s]) ? m.a_hi[s] : m.a_lo[s];
+      const double cv = a[0] - 1.0 + t * (a[1] + t * (a[2] + t * (a[3] + t * a[4])));
+      const double dcv = a[1] + t * (2.0 * a[2] + t * (3.0 * a[3] + t * 4.0 * a[4]));
+      if (cv > 0.0) {
+        const double k = 0.5 * (dcv < 0 ? -dcv : dcv) / cv;
+        if (k > kmax) kmax = k;
+      }
+    }
+  }
+  d.newton_k = kmax;
   return d;
 }
 
@@ -59,36 +75,6 @@ inline int upload_refops_local(int dim, int order, const double* packed64, const
   if (cudaMemcpyToSymbol(c_fnodes, fnodes, fn * sizeof(int), foff * sizeof(int)) != cudaSuccess)
     return MGC_E_CUDA;
   return MGC_OK;
-}
-
-// float copy of the device mechanism (every coefficient rounded to nearest)
-inline MechanismT<float> narrow_mechanism(const Mechanism& d) {
-  MechanismT<float> f;
-  memset(&f, 0, sizeof(f));
-  f.nspecies = d.nspecies;
-  f.nreactions = d.nreactions;
-  auto cp = [](float* dst, const double* src, int n) {
-    for (int i = 0; i < n; ++i) dst[i] = (float)src[i];
-  };
-  constexpr int S = MGC_MAX_SPECIES, R = MGC_MAX_REACTIONS;
-  cp(f.mw, d.mw, S);
-  cp(f.inv_mw, d.inv_mw, S);
-  cp(f.t_mid, d.t_mid, S);
-  cp(&f.a_lo[0][0], &d.a_lo[0][0], S * 7);
-  cp(&f.a_hi[0][0], &d.a_hi[0][0], S * 7);
-  cp(&f.ord_f[0][0], &d.ord_f[0][0], R * S);
-  cp(&f.nu_p[0][0], &d.nu_p[0][0], R * S);
-  cp(&f.nu_net[0][0], &d.nu_net[0][0], R * S);
-  cp(f.dnu, d.dnu, R);
-  cp(f.log_a, d.log_a, R);
-  cp(f.beta, d.beta, R);
-  cp(f.t_act, d.t_act, R);
-  for (int i = 0; i < R; ++i) f.reversible[i] = d.reversible[i];
-  cp(&f.h_lo[0][0], &d.h_lo[0][0], S * 6);
-  cp(&f.h_hi[0][0], &d.h_hi[0][0], S * 6);
-  cp(&f.s_lo[0][0], &d.s_lo[0][0], S * 6);
-  cp(&f.s_hi[0][0], &d.s_hi[0][0], S * 6);
-  return f;
 }
 
 inline int upload_mechanism_local(const Mechanism* m) {

@@ -307,40 +307,16 @@ __global__ void __launch_bounds__(256) k_mixture_state_mixed(
     float qq[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) qq[c] = q[(int64_t)c * nnodes + n];
-    const double irho = 1.0 / (double)qq[0];
-    float y[NS];
-    double yd[NS];
-#pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      yd[k] = (double)qq[2 + DIM + k] * irho;
-      y[k] = (float)yd[k];
-    }
-    double ked = 0;
-#pragma unroll
-    for (int i = 0; i < DIM; ++i) ked += (double)qq[2 + i] * (double)qq[2 + i];
-    const double e64 = ((double)qq[1] - 0.5 * ked * irho) * irho;
-    const float e32 = (float)e64;
+    float y[NS], e32;
+    double yd[NS], e64;
+    mixed_newton_inputs<DIM, NS>(qq, y, yd, e32, e64);
     int used = 0;
     float t = 0.f;
     bool ok = false;
     // attempt 0: learned guess (when given); attempt 1: the plain guess (seed)
     for (int attempt = tguess ? 0 : 1; attempt < 2 && !ok; ++attempt) {
       t = (attempt == 0) ? tguess[n] : tseed[n];
-      for (int it = 0; it < maxit; ++it) {
-        float em, cv;
-        mixture_e_cv<float, NS>(y, t, em, cv);
-        const float dt = (e32 - em) / cv;
-        t += dt;
-        ++used;
-        if (fabsf(dt) <= 1e-5f * fabsf(t)) break;
-      }
-      // float64 residual check; an accepted result takes the float64
-      // residual as its last Newton step
-      double em, cv;
-      mixture_e_cv<double, NS>(yd, (double)t, em, cv);
-      const double corr = (e64 - em) / cv;
-      ok = t > 0.f && fabs(corr / (double)t) <= (double)rtol;
-      if (ok) t = (float)((double)t + corr);
+      ok = mixed_newton<NS>(y, yd, e32, e64, t, maxit, (double)rtol, used);
       if (!ok && attempt == 0) used += 1000;
     }
     if (!ok) miss = true;

@@ -19,6 +19,7 @@ int tu2f_upload_refops(int, int, const double*, const float*, const int*);
 int tu3f_upload_refops(int, int, const double*, const float*, const int*);
 int tu2f_upload_mechanism(const Mechanism*);
 int tu3f_upload_mechanism(const Mechanism*);
+int mlp_upload_mechanism(const Mechanism*);
 int tu2f_dispatch(int, int, int, bool, const DGArgs<float>&, const GasParams&, cudaStream_t);
 int tu3f_dispatch(int, int, int, bool, const DGArgs<float>&, const GasParams&, cudaStream_t);
 int tu2f_mixture_state(int, int64_t, const float*, const float*, const float*, float*, int32_t*,
@@ -286,6 +287,8 @@ int mgc_set_mechanism(const mgc_mechanism_t* mech_host) {
   rc = tu2f_upload_mechanism(&m);
   if (rc) return rc;
   rc = tu3f_upload_mechanism(&m);
+  if (rc) return rc;
+  rc = mlp_upload_mechanism(&m);
   if (rc) return rc;
   rc = upload_mechanism_local(&m);
   if (rc) return rc;

@@ -29,6 +29,8 @@
 
 namespace {
 
+using namespace mgc;
+
 constexpr int H = 64;       // hidden width
 constexpr int KIN = 16;     // input features padded to one k-step
 constexpr int W2S = 72;     // padded bf16 row stride of W2 / W2^T in shared memory
@@ -45,6 +47,18 @@ constexpr int NPARAM = P_B3 + 1;
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// tanh x = 1 - 2 / (exp(2x) + 1), with exp(2x) = 2^(2x / ln 2) from the
+// ex2.approx instruction and the reciprocal from rcp.approx: about 2e-7
+// absolute error (far below the bf16 spacing of the activations), two
+// special-function operations, no cancellation issue at large |x| (the
+// quotient tends to 0 or 2).
+__device__ __forceinline__ float tanh_fast(float x) {
+  float e, r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(x * 2.8853900817779268f));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e + 1.0f));
+  return fmaf(-2.0f, r, 1.0f);
 }
 
 __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
@@ -114,10 +128,10 @@ __device__ __forceinline__ void forward_tile(const __nv_bfloat16* xs, const __nv
     const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + 2 * t + 8);
     mma_bf16(d, a0, a1, a2, a3, b0, b1);
     const float bb0 = bias[nt * 8 + 2 * t], bb1 = bias[nt * 8 + 2 * t + 1];
-    tl.h1[nt][0] = tanhf(d[0] + bb0);
-    tl.h1[nt][1] = tanhf(d[1] + bb1);
-    tl.h1[nt][2] = tanhf(d[2] + bb0);
-    tl.h1[nt][3] = tanhf(d[3] + bb1);
+    tl.h1[nt][0] = tanh_fast(d[0] + bb0);
+    tl.h1[nt][1] = tanh_fast(d[1] + bb1);
+    tl.h1[nt][2] = tanh_fast(d[2] + bb0);
+    tl.h1[nt][3] = tanh_fast(d[3] + bb1);
   }
   // layer 2: A = H1 (16 x 64) re-packed from the accumulators, B = W2^T
 #pragma unroll
@@ -135,10 +149,10 @@ __device__ __forceinline__ void forward_tile(const __nv_bfloat16* xs, const __nv
       mma_bf16(d, x0, x1, x2, x3, b0, b1);
     }
     const float bb0 = bias[H + nt * 8 + 2 * t], bb1 = bias[H + nt * 8 + 2 * t + 1];
-    tl.h2[nt][0] = tanhf(d[0] + bb0);
-    tl.h2[nt][1] = tanhf(d[1] + bb1);
-    tl.h2[nt][2] = tanhf(d[2] + bb0);
-    tl.h2[nt][3] = tanhf(d[3] + bb1);
+    tl.h2[nt][0] = tanh_fast(d[0] + bb0);
+    tl.h2[nt][1] = tanh_fast(d[1] + bb1);
+    tl.h2[nt][2] = tanh_fast(d[2] + bb0);
+    tl.h2[nt][3] = tanh_fast(d[3] + bb1);
   }
   // layer 3 (float32): partial dot products, reduced over the 4 lanes of a row
   float s0 = 0.f, s1 = 0.f;
@@ -154,6 +168,55 @@ __device__ __forceinline__ void forward_tile(const __nv_bfloat16* xs, const __nv
   s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
   tl.y0 = s0 + bias[3 * H];
   tl.y1 = s1 + bias[3 * H];
+}
+
+// Inference-only forward pass of one 16-sample tile: the same arithmetic as
+// forward_tile, with the layer-1 activations kept only as the packed bf16
+// pairs that form the layer-2 A fragments and the output layer accumulated
+// per layer-2 n-tile, so no activation array stays live.  Lanes with
+// lane % 4 == 0 hold y[g], y[g+8] in y0, y1.
+__device__ __forceinline__ void forward_tile_y(const __nv_bfloat16* xs,
+                                               const __nv_bfloat16* w1s,
+                                               const __nv_bfloat16* w2s, const float* bias,
+                                               float& y0, float& y1) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  constexpr int XS = KIN + 8;
+  const uint32_t a0 = *reinterpret_cast<const uint32_t*>(xs + g * XS + 2 * t);
+  const uint32_t a1 = *reinterpret_cast<const uint32_t*>(xs + (g + 8) * XS + 2 * t);
+  const uint32_t a2 = *reinterpret_cast<const uint32_t*>(xs + g * XS + 2 * t + 8);
+  const uint32_t a3 = *reinterpret_cast<const uint32_t*>(xs + (g + 8) * XS + 2 * t + 8);
+  uint32_t hp[8][2];
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    const __nv_bfloat16* wr = w1s + (nt * 8 + g) * (KIN + 8);
+    mma_bf16(d, a0, a1, a2, a3, *reinterpret_cast<const uint32_t*>(wr + 2 * t),
+             *reinterpret_cast<const uint32_t*>(wr + 2 * t + 8));
+    const float bb0 = bias[nt * 8 + 2 * t], bb1 = bias[nt * 8 + 2 * t + 1];
+    hp[nt][0] = pack_bf16(tanh_fast(d[0] + bb0), tanh_fast(d[1] + bb1));
+    hp[nt][1] = pack_bf16(tanh_fast(d[2] + bb0), tanh_fast(d[3] + bb1));
+  }
+  float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    const __nv_bfloat16* wr = w2s + (nt * 8 + g) * W2S;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk)
+      mma_bf16(d, hp[2 * kk][0], hp[2 * kk][1], hp[2 * kk + 1][0], hp[2 * kk + 1][1],
+               *reinterpret_cast<const uint32_t*>(wr + kk * 16 + 2 * t),
+               *reinterpret_cast<const uint32_t*>(wr + kk * 16 + 2 * t + 8));
+    const float bb0 = bias[H + nt * 8 + 2 * t], bb1 = bias[H + nt * 8 + 2 * t + 1];
+    const float w0 = bias[2 * H + nt * 8 + 2 * t], w1v = bias[2 * H + nt * 8 + 2 * t + 1];
+    s0 += w0 * tanh_fast(d[0] + bb0) + w1v * tanh_fast(d[1] + bb1);
+    s1 += w0 * tanh_fast(d[2] + bb0) + w1v * tanh_fast(d[3] + bb1);
+  }
+  s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+  s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
+  s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+  s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+  y0 = s0 + bias[3 * H];
+  y1 = s1 + bias[3 * H];
 }
 
 constexpr int WARPS = 4;
@@ -199,13 +262,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_mlp_infer(int64_t n, const float
       }
     }
     __syncwarp();
-    Tile tl;
-    forward_tile(xs, w1s, w2s, bias, tl);
+    float y0, y1;
+    forward_tile_y(xs, w1s, w2s, bias, y0, y1);
     if ((lane & 3) == 0) {
       const int g = lane >> 2;
       const int64_t s0 = tile * 16 + g, s1 = s0 + 8;
-      if (s0 < n) tout[s0] = net.out_shift + net.out_scale * tl.y0;
-      if (s1 < n) tout[s1] = net.out_shift + net.out_scale * tl.y1;
+      if (s0 < n) tout[s0] = net.out_shift + net.out_scale * y0;
+      if (s1 < n) tout[s1] = net.out_shift + net.out_scale * y1;
     }
     __syncwarp();
   }
@@ -469,7 +532,113 @@ int grid_for(int64_t tiles) {
   return nb < 1 ? 1 : (int)nb;
 }
 
+// {{{ mixture temperature with the learned guess (fused)
+
+// One warp per 32 nodes: the network runs on the warp's two 16-sample tiles
+// (features from the node's float64 energy and mass fractions), the guesses
+// go through shared memory, and each lane then solves its node's
+// temperature with mixed_newton from the guess, falling back to the seed
+// when the float64 residual check fails (iteration count + 1000 marks it).
+template <int DIM, int NS>
+__global__ void __launch_bounds__(WARPS * 32) k_mixture_state_learned(
+    int64_t n, const float* __restrict__ q, const float* __restrict__ tseed, Net net,
+    float* __restrict__ tout, int32_t* __restrict__ iters, int maxit, double rtol,
+    int32_t* __restrict__ status) {
+  __shared__ __align__(16) __nv_bfloat16 w1s[H * (KIN + 8)];
+  __shared__ __align__(16) __nv_bfloat16 w2s[H * W2S];
+  __shared__ float bias[3 * H + 1];
+  __shared__ __align__(16) __nv_bfloat16 xs_all[WARPS][32 * (KIN + 8)];
+  __shared__ float tg_all[WARPS][32];
+  stage_weights(net, w1s, w2s, nullptr, bias);
+  stage_bias(net, bias);
+  __syncthreads();
+  constexpr int NC = DIM + 2 + NS;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __nv_bfloat16* xs = xs_all[warp];
+  float* tg = tg_all[warp];
+  bool miss = false;
+  const int64_t nchunks = (n + 31) / 32;
+  for (int64_t ch = (int64_t)blockIdx.x * WARPS + warp; ch < nchunks;
+       ch += (int64_t)gridDim.x * WARPS) {
+    const int64_t s = ch * 32 + lane;
+    const bool valid = s < n;
+    // the Newton inputs are derived twice (features here, the solve after the
+    // network: the second read of q hits L1) so that none stays live across
+    // the network
+    {
+      float qq[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) qq[c] = valid ? q[(int64_t)c * n + s] : (c == 0 ? 1.f : 0.f);
+      float y[NS], e32;
+      double yd[NS], e64;
+      mixed_newton_inputs<DIM, NS>(qq, y, yd, e32, e64);
+      float f[8];
+      f[0] = e32;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) f[1 + k] = k < NS ? y[k] : 0.f;
+#pragma unroll
+      for (int j = 0; j < KIN; j += 2) {
+        const float v0 = j < 8 ? (f[j] - net.in_shift[j]) * net.in_scale[j] : 0.f;
+        const float v1 = j + 1 < 8 ? (f[j + 1] - net.in_shift[j + 1]) * net.in_scale[j + 1] : 0.f;
+        *reinterpret_cast<uint32_t*>(xs + lane * (KIN + 8) + j) = pack_bf16(v0, v1);
+      }
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int half = 0; half < 2; ++half) {
+      float y0, y1;
+      forward_tile_y(xs + half * 16 * (KIN + 8), w1s, w2s, bias, y0, y1);
+      if ((lane & 3) == 0) {
+        const int g = lane >> 2;
+        tg[half * 16 + g] = net.out_shift + net.out_scale * y0;
+        tg[half * 16 + g + 8] = net.out_shift + net.out_scale * y1;
+      }
+    }
+    __syncwarp();
+    if (valid) {
+      float qq[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) qq[c] = q[(int64_t)c * n + s];
+      float y[NS], e32;
+      double yd[NS], e64;
+      mixed_newton_inputs<DIM, NS>(qq, y, yd, e32, e64);
+      int used = 0;
+      float t = tg[lane];
+      bool ok = mixed_newton<NS>(y, yd, e32, e64, t, maxit, rtol, used);
+      if (!ok) {
+        used += 1000;
+        t = tseed[s];
+        ok = mixed_newton<NS>(y, yd, e32, e64, t, maxit, rtol, used);
+      }
+      if (!ok) miss = true;
+      tout[s] = t;
+      if (iters) iters[s] = used;
+    }
+    __syncwarp();
+  }
+  if (miss) atomicOr(status, ST_NEWTON_MISS);
+}
+
+// }}}
+
+bool g_mech_ready_mlp[64] = {};
+
 }  // namespace
+
+namespace mgc {
+
+// this unit's copy of the mechanism tables (mgc_set_mechanism)
+int mlp_upload_mechanism(const Mechanism* m) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MGC_E_CUDA;
+  if (cudaMemcpyToSymbol(c_mech, m, sizeof(Mechanism)) != cudaSuccess) return MGC_E_CUDA;
+  const MechanismT<float> f = narrow_mechanism(*m);
+  if (cudaMemcpyToSymbol(c_mech32, &f, sizeof(f)) != cudaSuccess) return MGC_E_CUDA;
+  g_mech_ready_mlp[dev] = true;
+  return MGC_OK;
+}
+
+}  // namespace mgc
 
 extern "C" {
 
@@ -532,6 +701,33 @@ int mgc_mlp_adam(const mgc_mlp_t* w, const float* grad, float* m, float* v, floa
       w->params, grad, m, v, lr, beta1, beta2, eps, bc1, bc2,
       reinterpret_cast<__nv_bfloat16*>(w->w1_bf16), reinterpret_cast<__nv_bfloat16*>(w->w2_bf16),
       reinterpret_cast<__nv_bfloat16*>(w->w2t_bf16));
+  return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+}
+
+int mgc_mixture_temperature_learned_f32(int dim, const mgc_gas_t* gas, int64_t nnodes,
+                                        const float* q, const float* t_seed,
+                                        const mgc_mlp_t* mlp, float* t_out,
+                                        int32_t* iterations, int maxit, float rtol,
+                                        int32_t* status, void* stream) {
+  if (!gas || gas->eos_kind != MGC_EOS_MIXTURE || gas->nspecies != 7 || !mlp_ok(mlp) ||
+      nnodes < 0 || !q || !t_seed || !t_out || !status || maxit < 1 || !(rtol > 0.f) ||
+      (dim != 2 && dim != 3))
+    return MGC_E_INVALID;
+  if (nnodes == 0) return MGC_OK;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MGC_E_CUDA;
+  if (!g_mech_ready_mlp[dev]) return MGC_E_NOT_READY;
+  const Net net = make_net(mlp);
+  const int nb = grid_for((nnodes + 31) / 32);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dim == 3)
+    k_mixture_state_learned<3, 7><<<nb, WARPS * 32, 0, s>>>(nnodes, q, t_seed, net, t_out,
+                                                             iterations, maxit, (double)rtol,
+                                                             status);
+  else
+    k_mixture_state_learned<2, 7><<<nb, WARPS * 32, 0, s>>>(nnodes, q, t_seed, net, t_out,
+                                                             iterations, maxit, (double)rtol,
+                                                             status);
   return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
 }
 

@@ -17,6 +17,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #define MGC_MAX_SPECIES 16
 #define MGC_MAX_REACTIONS 8
 
@@ -66,6 +68,10 @@ struct MechanismT {
   // and entropy coefficients (a0, a1, a2/2, a3/3, a4/4, a6), low / high range
   T h_lo[MGC_MAX_SPECIES][6], h_hi[MGC_MAX_SPECIES][6];
   T s_lo[MGC_MAX_SPECIES][6], s_hi[MGC_MAX_SPECIES][6];
+  // derived at upload: bound on |c_v'(T)| / (2 c_v(T)) (1/K) over the
+  // species and the NASA-7 temperature range, the quadratic-convergence
+  // constant of the temperature Newton iteration
+  T newton_k;
 };
 using Mechanism = MechanismT<double>;
 
@@ -76,6 +82,37 @@ static __constant__ MechanismT<float> c_mech32;
 template <class R> __device__ __forceinline__ const MechanismT<R>& mech();
 template <> __device__ __forceinline__ const MechanismT<double>& mech<double>() { return c_mech; }
 template <> __device__ __forceinline__ const MechanismT<float>& mech<float>() { return c_mech32; }
+
+// float copy of the device mechanism (every coefficient rounded to nearest)
+static inline MechanismT<float> narrow_mechanism(const Mechanism& d) {
+  MechanismT<float> f;
+  memset(&f, 0, sizeof(f));
+  f.nspecies = d.nspecies;
+  f.nreactions = d.nreactions;
+  auto cp = [](float* dst, const double* src, int n) {
+    for (int i = 0; i < n; ++i) dst[i] = (float)src[i];
+  };
+  constexpr int S = MGC_MAX_SPECIES, R = MGC_MAX_REACTIONS;
+  cp(f.mw, d.mw, S);
+  cp(f.inv_mw, d.inv_mw, S);
+  cp(f.t_mid, d.t_mid, S);
+  cp(&f.a_lo[0][0], &d.a_lo[0][0], S * 7);
+  cp(&f.a_hi[0][0], &d.a_hi[0][0], S * 7);
+  cp(&f.ord_f[0][0], &d.ord_f[0][0], R * S);
+  cp(&f.nu_p[0][0], &d.nu_p[0][0], R * S);
+  cp(&f.nu_net[0][0], &d.nu_net[0][0], R * S);
+  cp(f.dnu, d.dnu, R);
+  cp(f.log_a, d.log_a, R);
+  cp(f.beta, d.beta, R);
+  cp(f.t_act, d.t_act, R);
+  for (int i = 0; i < R; ++i) f.reversible[i] = d.reversible[i];
+  cp(&f.h_lo[0][0], &d.h_lo[0][0], S * 6);
+  cp(&f.h_hi[0][0], &d.h_hi[0][0], S * 6);
+  cp(&f.s_lo[0][0], &d.s_lo[0][0], S * 6);
+  cp(&f.s_hi[0][0], &d.s_hi[0][0], S * 6);
+  f.newton_k = (float)d.newton_k;
+  return f;
+}
 
 constexpr double kGasConstant = 8314.46261815324;
 constexpr double kOneAtm = 101325.0;
@@ -214,6 +251,57 @@ __device__ __forceinline__ R newton_temperature(R e, R tguess, const R* y, int n
     t = t + (e - em) / cv;
   }
   return t;
+}
+
+// Newton inputs of the mixed form from a float32 conserved state: mass
+// fractions and specific internal energy in float64 (one reciprocal of rho)
+// and their float32 roundings.
+template <int DIM, int NS>
+__device__ __forceinline__ void mixed_newton_inputs(const float* qq, float* y, double* yd,
+                                                    float& e32, double& e64) {
+  const double irho = 1.0 / (double)qq[0];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    yd[k] = (double)qq[2 + DIM + k] * irho;
+    y[k] = (float)yd[k];
+  }
+  double ked = 0;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) ked += (double)qq[2 + i] * (double)qq[2 + i];
+  e64 = ((double)qq[1] - 0.5 * ked * irho) * irho;
+  e32 = (float)e64;
+}
+
+// Mixed-precision temperature solve of one node from the start value *t*.
+// Newton converges quadratically: after a step dT the remaining error is
+// about k dT^2, k = max |c_v'| / (2 c_v) (Mechanism::newton_k).  The float32
+// iterations stop once that predicted error is a quarter of the error the
+// final float64 step can absorb; the float64 residual then gives the last
+// correction, accepted when its own predicted remainder k corr^2 is at most
+// rtol |T| (the relative temperature-update tolerance the reference drivers
+// check: mirgecom examples/autoignition.py:526-530).  Returns acceptance;
+// *used* counts float32 iterations.
+template <int NS>
+__device__ __forceinline__ bool mixed_newton(const float* y, const double* yd, float e32,
+                                             double e64, float& t, int maxit, double rtol,
+                                             int& used) {
+  const float k = mech<float>().newton_k;
+  const float rt = (float)rtol;
+  for (int it = 0; it < maxit; ++it) {
+    float em, cv;
+    mixture_e_cv<float, NS>(y, t, em, cv);
+    const float dt = (e32 - em) / cv;
+    t += dt;
+    ++used;
+    if (k * dt * dt <= 0.25f * sqrtf(rt * fabsf(t) / k)) break;
+  }
+  double em, cv;
+  mixture_e_cv<double, NS>(yd, (double)t, em, cv);
+  const double corr = (e64 - em) / cv;
+  const bool ok = t > 0.f && corr == corr &&
+                  mech<double>().newton_k * corr * corr <= rtol * fabs((double)t);
+  if (ok) t = (float)((double)t + corr);
+  return ok;
 }
 
 // net molar production rates (kmol/m^3/s)

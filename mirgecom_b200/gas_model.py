@@ -117,9 +117,9 @@ def make_fluid_state(cv: ConservedVars, gas_model: GasModel, temperature_seed=No
     if cv.q.dtype == torch.float32:
         # mixed form: learned guess (if the EOS carries one), float32 Newton
         # with adaptive stop, float64 residual check, plain-guess fallback
-        guess = eos.learned_temperature_guess(cv) if eos.learned_guess is not None else None
-        t = runtime.mixture_temperature_mixed(cv, gas_model, tseed, guess,
-                                              iters=kwargs.get("newton_iterations"))
+        t = runtime.mixture_temperature_mixed(cv, gas_model, tseed,
+                                              iters=kwargs.get("newton_iterations"),
+                                              learned=eos.learned_guess)
         return FluidState(cv, gas_model, temperature=t, operator_temperature=t)
     t1, t2 = runtime.mixture_temperature(cv, gas_model, tseed)
     return FluidState(cv, gas_model, temperature=t1, operator_temperature=t2)

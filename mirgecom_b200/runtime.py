@@ -120,13 +120,19 @@ def _gas_struct(gas_model, nspecies, device):
     return gas_model.to_struct(nspecies)
 
 
+# float32 iteration cap per start value; relative temperature-update
+# tolerance of the accepted result (the convergence check of the reference
+# drivers, mirgecom examples/autoignition.py:526-530)
 MIXED_NEWTON_MAXIT = 12
-MIXED_NEWTON_RTOL = 1e-3
+MIXED_NEWTON_RTOL = 1e-8
 
 
-def mixture_temperature_mixed(cv, gas_model, tseed, tguess=None, iters=None, status=None):
-    """Mixed-form temperature: float32 Newton from *tguess* (else *tseed*),
-    float64 residual check, plain-guess fallback.  Returns T (float32)."""
+def mixture_temperature_mixed(cv, gas_model, tseed, tguess=None, iters=None, status=None,
+                              learned=None):
+    """Mixed-form temperature: float32 Newton from the learned guess (*learned*,
+    a TemperatureMLP evaluated in the same kernel, or a precomputed *tguess*)
+    else from *tseed*, float64 residual check, plain-guess fallback.  Returns
+    T (float32)."""
     q = cv.q
     _lib.require_cuda(q)
     lib = _lib.load()
@@ -139,10 +145,17 @@ def mixture_temperature_mixed(cv, gas_model, tseed, tguess=None, iters=None, sta
     if status is None:
         status = torch.zeros(1, dtype=torch.int32, device=q.device)
     with torch.cuda.device(q.device):
-        _lib.check(lib.mgc_mixture_temperature_f32(
-            cv.dim, C.byref(gs), n, _lib.ptr(q), _lib.ptr(tseed), _lib.ptr(tguess),
-            _lib.ptr(tout), _lib.ptr(iters), MIXED_NEWTON_MAXIT, MIXED_NEWTON_RTOL,
-            _lib.ptr(status), _lib.stream_handle()), "mgc_mixture_temperature_f32")
+        if learned is not None:
+            ms = learned.struct()
+            _lib.check(lib.mgc_mixture_temperature_learned_f32(
+                cv.dim, C.byref(gs), n, _lib.ptr(q), _lib.ptr(tseed), C.byref(ms),
+                _lib.ptr(tout), _lib.ptr(iters), MIXED_NEWTON_MAXIT, MIXED_NEWTON_RTOL,
+                _lib.ptr(status), _lib.stream_handle()), "mgc_mixture_temperature_learned_f32")
+        else:
+            _lib.check(lib.mgc_mixture_temperature_f32(
+                cv.dim, C.byref(gs), n, _lib.ptr(q), _lib.ptr(tseed), _lib.ptr(tguess),
+                _lib.ptr(tout), _lib.ptr(iters), MIXED_NEWTON_MAXIT, MIXED_NEWTON_RTOL,
+                _lib.ptr(status), _lib.stream_handle()), "mgc_mixture_temperature_f32")
     return tout
 
 
