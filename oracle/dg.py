@@ -179,6 +179,24 @@ def div_operator(disc, v, flux):
     return -disc.inverse_mass(disc.weak_local_div(v) - disc.face_mass(flux))
 
 
+def scalar_gradient(disc, u, exact):
+    """Weak gradient of a scalar with the central flux on interior faces and
+    the exact value *exact(x)* on boundary faces (the set-up of
+    test/test_operators.py:208-228 and :330-417)."""
+    nrm = _face_normals(disc)
+    avg = ph.num_flux_central(disc.to_faces(u), disc.exterior(u))
+    flux = np.array([avg * nrm[j] for j in range(disc.dim)])
+    flux = flux * disc.interior_mask[None, :, :, None]
+    be, bf = disc.bface_elem, disc.bface_face
+    xb = disc.nodes[:, be[:, None], disc.refel.face_nodes[bf]]
+    ub = exact(xb)                                        # (nbf, Nfp)
+    bn = _bnormals(disc)
+    mask = np.ones(len(be), dtype=bool)
+    for j in range(disc.dim):
+        flux[j] = flux[j] + _scatter_boundary(disc, ub * bn[j], flux[j].shape, mask)
+    return grad_operator(disc, u, flux)
+
+
 # {{{ boundaries (mirgecom/boundary.py)
 
 class DummyBoundary:

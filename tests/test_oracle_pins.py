@@ -1,0 +1,219 @@
+"""Pins of the CPU oracle against the reference's own known-answer tests.
+
+The reference's runtime (grudge/meshmode/pyopencl, pyrometheus/cantera) is
+absent, so the oracle's agreement with the reference is pinned through the
+analytic checks the reference's test suite makes, restated here on the
+oracle, plus identities of the thermochemistry that its Cantera-based tests
+rely on.  CPU only; sized to run in well under a minute.
+"""
+
+import re
+
+import numpy as np
+import pytest
+
+from cases import make_disc, vortex_np
+from mirgecom_b200.thermochemistry import GAS_CONSTANT, UIUC_7SP
+from oracle import dg as odg
+from oracle import physics as oph
+
+
+def _uniform_q(dim, nspecies, shape):
+    """test/test_euler.py:121-136: rho = 1, rho E = 2.5, v = 0,
+    Y_i = 1 / (10 (i + 1))."""
+    q = np.zeros((dim + 2 + nspecies,) + shape)
+    q[0] = 1.0
+    q[1] = 2.5
+    for i in range(nspecies):
+        q[2 + dim + i] = 1.0 / ((i + 1) * 10)
+    return q
+
+
+@pytest.mark.parametrize("dim,order", [(2, 1), (2, 3), (3, 1), (3, 2)])
+@pytest.mark.parametrize("nspecies", [0, 3])
+@pytest.mark.parametrize("flux", ["rusanov", "hll"])
+def test_uniform_state_euler_rhs_vanishes(dim, order, nspecies, flux):
+    """test/test_euler.py:87-236: a uniform state gives rhs = 0 to FP."""
+    _, od = make_disc("simplex", dim, 3, order, (-0.5,) * dim, (0.5,) * dim, True)
+    q = _uniform_q(dim, nspecies, od.nodes.shape[1:])
+    gas = oph.IdealGas()
+    st = oph.make_fluid_state(q, gas, None, dim)
+    rhs = odg.euler_operator(od, st, gas, {}, flux=flux)
+    assert np.abs(rhs).max() < 1e-9
+
+
+@pytest.mark.parametrize("dim,order", [(2, 2), (3, 1)])
+def test_uniform_state_ns_rhs_vanishes(dim, order):
+    """test/test_navierstokes.py:86-225: uniform state, viscous terms on."""
+    _, od = make_disc("simplex", dim, 3, order, (-0.5,) * dim, (0.5,) * dim, True)
+    q = _uniform_q(dim, 2, od.nodes.shape[1:])
+    gas = oph.IdealGas()
+    tr = oph.SimpleTransportParams(viscosity=1e-2, thermal_conductivity=1e-2,
+                                   species_diffusivity=(1e-2, 2e-2))
+    st = oph.make_fluid_state(q, gas, tr, dim)
+    rhs = odg.ns_operator(od, st, gas, tr, {})
+    assert np.abs(rhs).max() < 1e-9
+
+
+def _eoc(hs, errs):
+    return float(np.polyfit(np.log(hs), np.log(errs), 1)[0])
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_static_vortex_rhs_converges(order):
+    """test/test_euler.py:410-485: the static isentropic vortex is a steady
+    solution, so rhs -> 0 at order >= p - 0.7 with exact boundary states."""
+    hs, errs = [], []
+    for n in (24, 32, 48):
+        _, od = make_disc("simplex", 2, n, order, (-5.0, -5.0), (5.0, 5.0), False)
+        q = vortex_np(od.nodes, center=(0.0, 0.0), vel=(0.0, 0.0))
+        gas = oph.IdealGas()
+        st = oph.make_fluid_state(q, gas, None, 2)
+        bnd = {"all": odg.PrescribedBoundary(
+            lambda x, t: vortex_np(x, t, center=(0.0, 0.0), vel=(0.0, 0.0)))}
+        rhs = odg.euler_operator(od, st, gas, bnd)
+        hs.append(10.0 / n)
+        errs.append(np.abs(rhs).max())
+    assert _eoc(hs, errs) >= order - 0.7, (hs, errs)
+
+
+@pytest.mark.parametrize("dim,order", [(2, 1), (2, 3), (3, 2)])
+def test_gradient_exact_for_polynomials(dim, order):
+    """test/test_operators.py:257-417 (coordinate functions of degree <= p):
+    the DG gradient with central fluxes and exact boundary values is exact."""
+    _, od = make_disc("simplex", dim, 3, order, (0.0,) * dim, (1.0, 2.0, 4.0)[:dim], False)
+    x = od.nodes
+
+    def power(j):
+        return min(order, 2 if j == 0 else 1)
+
+    def exact(xx):
+        return sum((j + 1) * xx[j] ** power(j) for j in range(dim))
+
+    g = odg.scalar_gradient(od, exact(x), exact)
+    ge = np.zeros_like(g)
+    for j in range(dim):
+        ge[j] = (j + 1) * power(j) * x[j] ** (power(j) - 1)
+    assert np.abs(g - ge).max() < 1e-10 * max(1.0, np.abs(ge).max())
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_gradient_of_trig_function_converges(order):
+    """test/test_operators.py:257-417 (_trig_test_func): order >= p - 0.5."""
+    hs, errs = [], []
+    for n in (4, 6, 8):
+        _, od = make_disc("simplex", 2, n, order, (0.0, 0.0), (1.0, 2.0), False)
+        x = od.nodes
+
+        def f(xx):
+            return np.sin(2 * np.pi * xx[0]) * np.cos(np.pi * xx[1] / 2.0)
+
+        g = odg.scalar_gradient(od, f(x), f)
+        gx = 2 * np.pi * np.cos(2 * np.pi * x[0]) * np.cos(np.pi * x[1] / 2)
+        gy = -np.pi / 2 * np.sin(2 * np.pi * x[0]) * np.sin(np.pi * x[1] / 2)
+        hs.append(1.0 / n)
+        errs.append(max(np.abs(g[0] - gx).max(), np.abs(g[1] - gy).max()))
+    assert _eoc(hs, errs) >= order - 0.5, (hs, errs)
+
+
+@pytest.mark.parametrize("flux", ["rusanov", "hll", "central"])
+def test_numerical_flux_consistency(flux):
+    """test/test_inviscid.py:281-370: F*(q, q) = F(q) . n for each flux."""
+    rng = np.random.default_rng(0)
+    dim, ns = 3, 2
+    q = np.empty((dim + 2 + ns, 50))
+    q[0] = rng.uniform(0.5, 2.0, 50)
+    vel = rng.uniform(-1, 1, (dim, 50))
+    p = rng.uniform(0.5, 2.0, 50)
+    q[2:2 + dim] = q[0] * vel
+    q[1] = p / 0.4 + 0.5 * q[0] * (vel * vel).sum(axis=0)
+    q[2 + dim:] = q[0] * rng.uniform(0, 1, (ns, 50))
+    n = rng.normal(size=(dim, 50))
+    n /= np.linalg.norm(n, axis=0)
+    gas = oph.IdealGas()
+    st = oph.make_fluid_state(q, gas, None, dim)
+    fn = {"rusanov": oph.inviscid_facial_flux_rusanov, "hll": oph.inviscid_facial_flux_hll,
+          "central": oph.inviscid_facial_flux_central}[flux](st, st, n)
+    ref = oph.dot_normal(oph.inviscid_flux(st), n)
+    assert np.abs(fn - ref).max() < 1e-13 * np.abs(ref).max()
+
+
+# {{{ thermochemistry identities (the reference's versions need Cantera)
+
+def _random_mixture(n, seed):
+    rng = np.random.default_rng(seed)
+    t = rng.uniform(300.0, 2500.0, n)
+    y = rng.dirichlet([2.0] * UIUC_7SP.nspecies, n).T
+    return t, y
+
+
+def test_temperature_round_trip():
+    """test/test_eos.py:406-452 restated: T(e(T)) = T from a perturbed guess."""
+    t, y = _random_mixture(2000, 1)
+    e = oph.mixture_e_mass(UIUC_7SP, t, y)
+    guess = t + np.random.default_rng(2).uniform(-50, 50, t.shape)
+    tn = oph.newton_temperature(UIUC_7SP, e, guess, y, 5)
+    assert np.abs(tn - t).max() / t.min() < 1e-12
+
+
+def test_source_terms_conserve_mass():
+    """sum_k W_k omega_k = 0 (the mass check of test/test_chemistry.py)."""
+    t, y = _random_mixture(500, 3)
+    rho = np.random.default_rng(4).uniform(0.1, 1.5, t.shape)
+    om = oph.net_production_rates(UIUC_7SP, rho, t, y)
+    w = UIUC_7SP.molecular_weights[:, None]
+    scale = np.abs(w * om).max(axis=0) + 1e-300
+    assert (np.abs((w * om).sum(axis=0)) / scale).max() < 1e-12
+
+
+def _composition(name):
+    return {el: int(c or 1) for el, c in re.findall(r"([A-Z][a-z]?)(\d*)", name)}
+
+
+def test_source_terms_conserve_elements():
+    t, y = _random_mixture(500, 5)
+    rho = np.random.default_rng(6).uniform(0.1, 1.5, t.shape)
+    om = oph.net_production_rates(UIUC_7SP, rho, t, y)
+    comp = [_composition(s) for s in UIUC_7SP.species]
+    for el in ("C", "H", "O", "N"):
+        a = np.array([c.get(el, 0) for c in comp], dtype=np.float64)[:, None]
+        scale = np.abs(a * om).max(axis=0) + 1e-300
+        assert (np.abs((a * om).sum(axis=0)) / scale).max() < 1e-12, el
+
+
+def test_nasa7_continuous_at_midpoint():
+    """Both NASA-7 ranges agree at T_mid (cp, h, s) to the fits' precision."""
+    mech = UIUC_7SP
+    for k in range(mech.nspecies):
+        tm = mech.t_mid[k]
+        lo = np.array([tm * (1 - 1e-12)])
+        hi = np.array([tm * (1 + 1e-12)])
+        for fn in (oph.species_cp_r, oph.species_h_rt, oph.species_s_r):
+            a, b = fn(mech, lo)[k], fn(mech, hi)[k]
+            assert abs(a - b) <= 2e-3 * max(abs(a), 1.0), (mech.species[k], fn.__name__, a, b)
+
+
+def test_reversible_rate_vanishes_at_equilibrium():
+    """Detailed balance: concentrations with [CO2] / ([CO][O2]^(1/2)) = K_c
+    give equal forward and reverse rates for the reversible reaction."""
+    mech = UIUC_7SP
+    i = int(np.flatnonzero(mech.reversible)[0])
+    t = np.array([1200.0, 1800.0, 2400.0])
+    nu = mech.nu_prod[i] - mech.nu_reac[i]
+    g_rt = oph.species_h_rt(mech, t) - oph.species_s_r(mech, t)
+    log_kc = -np.tensordot(nu, g_rt, axes=(0, 0)) + nu.sum() * np.log(
+        oph.ONE_ATM / (GAS_CONSTANT * t))
+    conc = np.full((mech.nspecies, t.size), 1e-3)
+    prod = np.flatnonzero(nu > 0)
+    assert len(prod) == 1
+    reac = np.flatnonzero(nu < 0)
+    log_q = sum(-nu[k] * np.log(conc[k]) for k in reac)
+    conc[prod[0]] = np.exp((log_kc + log_q) / nu[prod[0]])
+    kf = np.exp(mech.log_a[i] + mech.beta[i] * np.log(t) - mech.t_act[i] / t)
+    rf = kf * np.prod([conc[k] ** mech.orders_fwd[i, k] for k in range(mech.nspecies)],
+                      axis=0)
+    rr = kf * np.exp(-log_kc) * np.prod(
+        [conc[k] ** mech.nu_prod[i, k] for k in range(mech.nspecies)], axis=0)
+    assert np.abs(rf - rr).max() < 1e-10 * rf.max()
+
+# }}}
