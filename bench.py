@@ -112,21 +112,33 @@ def build_workload(name, device):
     return dcoll, cv, gas, tseed
 
 
+KERNEL_NAMES = {"state": "k_mixture_state*", "grad": "k_grad", "node_flux": "k_node_flux",
+                "surface": "k_surface"}
+
+
 def algorithmic_bytes(dcoll, nc, s=8, mixture=False):
     """Compulsory HBM bytes per launch of each kernel of one NS RHS.
 
     state (mixture): read q (Nc) and the seed, write T (1, plus the operator
     temperature on the float64 path).  grad: read q (Nc) [+ T], write grad
-    ((Nc+1) d) per node.  rhs: read q (Nc) + grad ((Nc+1) d) [+ T, T_src],
-    write rhs (Nc) per node.  Plus rx and the face pairing per element.
+    ((Nc+1) d) per node.  node_flux: read q, grad [+ T, T_src], write the
+    flux record (FW values: Nc d fluxes, p, c, gamma, padded) [+ Ns
+    sources].  surface: read the records, q [+ sources], write the rhs (Nc).
+    rhs: the divergence pass as one (q + grad + rhs [+ 2 T] per node, no
+    records).  Plus rx and the face pairing per element where used.
     """
     d = dcoll.dim
     nn = dcoll.nelements * dcoll.refel.nnodes
     geo = dcoll.nelements * (d * d * s + dcoll.nfaces * 4)
     t_in = 1 if mixture else 0
-    grad = nn * (nc + t_in + (nc + 1) * d) * s + geo
-    rhs = nn * (nc + (nc + 1) * d + nc + 2 * t_in) * s + geo
-    out = {"grad": grad, "rhs": rhs}
+    ns = nc - d - 2
+    fw = -(-(nc * d + 3) // 4) * 4
+    out = {
+        "grad": nn * (nc + t_in + (nc + 1) * d) * s + geo,
+        "node_flux": nn * (nc + (nc + 1) * d + 2 * t_in + fw + (ns if mixture else 0)) * s,
+        "surface": nn * (fw + nc + (ns if mixture else 0) + nc) * s + geo,
+        "rhs": nn * (nc + (nc + 1) * d + nc + 2 * t_in) * s + geo,
+    }
     if mixture:
         out["state"] = nn * (nc + 1 + (2 if s == 8 else 1)) * s
     return out
@@ -192,12 +204,10 @@ def _dist_env():
     return rank, world, local
 
 
-def _oracle_sample(name):
-    """Oracle discretization and state on a bounded sample of the workload."""
-    import torch
-
+def _oracle_setup(name):
+    """Oracle discretization and gas of a bounded sample of the workload
+    (numpy only; no torch, so spawned CPU workers stay light)."""
     from mirgecom_b200.discretization import Discretization
-    from mirgecom_b200.initializers import reacting_mixture_state
     from mirgecom_b200.mesh import generate_box_mesh
     from mirgecom_b200.thermochemistry import UIUC_7SP
     from oracle import dg as odg
@@ -207,31 +217,37 @@ def _oracle_sample(name):
         n_sample = 6
         mesh = generate_box_mesh((-np.pi,) * 3, (np.pi,) * 3, (n_sample,) * 3,
                                  periodic=(True,) * 3)
+        mu = 1 / 1600
+        otr = oph.SimpleTransportParams(viscosity=mu, thermal_conductivity=mu * 1004.85 / 0.71)
+        gas = oph.IdealGas()
     else:
         n_sample = 3
         mesh = generate_box_mesh((0.0,) * 3, (2 * np.pi,) * 3, (n_sample,) * 3,
                                  periodic=(True,) * 3)
+        otr = oph.SimpleTransportParams(viscosity=1e-5, thermal_conductivity=1e-5,
+                                        species_diffusivity=(1e-5,) * 7)
+        gas = oph.MixtureGas(UIUC_7SP, temperature_niter=5)
     d = Discretization(mesh, w["order"])
     od = odg.OracleDisc(mesh, d.refel)
+    return od, gas, otr, mesh.nelements, n_sample
+
+
+def _oracle_state(name, od):
+    """The workload's state on the sample's nodes: (q, temperature seed)."""
+    w = WORKLOADS[name]
     x = od.nodes
     if w["kind"] == "tgv":
         u = np.sin(x[0]) * np.cos(x[1]) * np.cos(x[2])
         v = -np.cos(x[0]) * np.sin(x[1]) * np.cos(x[2])
         p = 1 / (1.4 * 0.01) + (np.cos(2 * x[0]) + np.cos(2 * x[1])) * (np.cos(2 * x[2]) + 2) / 16
         q = np.array([np.ones_like(u), p / 0.4 + 0.5 * (u * u + v * v), u, v, 0 * u])
-        mu = 1 / 1600
-        otr = oph.SimpleTransportParams(viscosity=mu, thermal_conductivity=mu * 1004.85 / 0.71)
-        gas = oph.IdealGas()
-        tseed = None
-    else:
-        cv, t = reacting_mixture_state([torch.from_numpy(x[i]) for i in range(3)],
-                                       UIUC_7SP, seed=0)
-        q = cv.q.numpy()
-        tseed = t.numpy() + 2.0
-        otr = oph.SimpleTransportParams(viscosity=1e-5, thermal_conductivity=1e-5,
-                                        species_diffusivity=(1e-5,) * 7)
-        gas = oph.MixtureGas(UIUC_7SP, temperature_niter=5)
-    return od, q, tseed, gas, otr, mesh.nelements, n_sample
+        return q, None
+    import torch
+
+    from mirgecom_b200.initializers import reacting_mixture_state
+    from mirgecom_b200.thermochemistry import UIUC_7SP
+    cv, t = reacting_mixture_state([torch.from_numpy(x[i]) for i in range(3)], UIUC_7SP, seed=0)
+    return cv.q.numpy(), t.numpy() + 2.0
 
 
 def _oracle_rhs(od, q, tseed, gas, otr):
@@ -244,10 +260,9 @@ def _oracle_rhs(od, q, tseed, gas, otr):
     return rhs
 
 
-def cpu_baseline(name, seconds=10.0):
-    """The float64 oracle (numpy, one host thread) on a bounded sample of the
-    same physics and order; the sample is stated in the result."""
-    od, q, tseed, gas, otr, nel, n_sample = _oracle_sample(name)
+def _time_oracle(name, q, tseed, seconds):
+    """RHS evaluations of the oracle on the sample for about *seconds*."""
+    od, gas, otr, nel, n_sample = _oracle_setup(name)
     _oracle_rhs(od, q, tseed, gas, otr)
     t0 = time.perf_counter()
     reps = 0
@@ -255,27 +270,59 @@ def cpu_baseline(name, seconds=10.0):
         _oracle_rhs(od, q, tseed, gas, otr)
         reps += 1
     dt = (time.perf_counter() - t0) / reps
-    dof = q.size
-    return {"value": dof / dt, "unit": "DOF-RHS/s", "cores": 1, "kind": "port",
-            "sample": f"{n_sample}^3 x 6 tets ({nel} tets, {dof} DOF), same physics and "
-                      f"order as {name}, {reps} RHS evaluations, numpy float64 oracle"}
+    return q.size / dt, reps, nel, n_sample
+
+
+def cpu_baseline(name, seconds=10.0):
+    """The float64 oracle (numpy, one process) on a bounded sample of the
+    same physics and order; the sample is stated in the result."""
+    od, _, _, _, _ = _oracle_setup(name)
+    q, tseed = _oracle_state(name, od)
+    value, reps, nel, n_sample = _time_oracle(name, q, tseed, seconds)
+    return {"value": value, "unit": "DOF-RHS/s", "cores": 1, "kind": "port",
+            "sample": f"{n_sample}^3 x 6 tets ({nel} tets, {q.size} DOF), same physics and "
+                      f"order as {name}, {reps} RHS evaluations, numpy float64 oracle, "
+                      f"one process"}
+
+
+def _reference_worker(job):
+    name, q, tseed, seconds = job
+    return _time_oracle(name, q, tseed, seconds)
 
 
 def run_reference(args):
+    """The reference's CPU path (restated by the oracle: the reference's own
+    runtime is not installed) on every host core: one spawned process per
+    core, each evaluating the RHS of the bounded sample; the value is the sum
+    of their rates."""
     rank, world, _ = _dist_env()
     if rank != 0:
         return
     t0 = time.perf_counter()
-    res = cpu_baseline(args.workload, seconds=max(5.0, 2.0 * args.steps))
-    line = {"impl": "reference", "metric": "DOF-RHS evals/s", "value": res["value"],
+    ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
+    od, _, _, _, _ = _oracle_setup(args.workload)
+    q, tseed = _oracle_state(args.workload, od)
+    seconds = max(5.0, 2.0 * args.steps)
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(ncores) as pool:
+        res = pool.map(_reference_worker, [(args.workload, q, tseed, seconds)] * ncores)
+    value = float(sum(r[0] for r in res))
+    reps = sum(r[1] for r in res)
+    _, _, nel, n_sample = res[0]
+    sample = (f"{n_sample}^3 x 6 tets ({nel} tets, {q.size} DOF), same physics and order "
+              f"as {args.workload}, {reps} RHS evaluations over {ncores} processes, numpy "
+              f"float64 oracle (the reference's CPU path restated; its runtime is not "
+              f"installed)")
+    line = {"impl": "reference", "metric": "DOF-RHS evals/s", "value": value,
             "unit": "DOF-RHS/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "sample": res["sample"]},
-            "cpu_baseline": {"value": res["value"], "unit": res["unit"],
-                             "cores": res["cores"], "kind": res["kind"],
-                             "sample": res["sample"]},
-            "e2e": {"value": res["value"], "unit": "DOF-RHS/s",
+            "config": {"workload": args.workload, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "DOF-RHS/s", "cores": ncores,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "DOF-RHS/s",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": time.perf_counter() - t0}
     print(json.dumps(line), flush=True)
@@ -303,14 +350,17 @@ def _time_form(dcoll, gas, q, tseed, steps, warmup, flush, stream):
     evs = []
     for i in range(steps):
         flush.fill_(float(i))
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        # start | state | grad | node_flux | surface
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         _rhs_call(dcoll, gas, q, tseed, events=ev)
         evs.append(ev)
     torch.cuda.synchronize()
-    step_ms = [e[0].elapsed_time(e[3]) for e in evs]
-    kern = {"state": float(np.mean([e[0].elapsed_time(e[1]) for e in evs])),
-            "grad": float(np.mean([e[1].elapsed_time(e[2]) for e in evs])),
-            "rhs": float(np.mean([e[2].elapsed_time(e[3]) for e in evs]))}
+    step_ms = [e[0].elapsed_time(e[4]) for e in evs]
+
+    def mean(i, j):
+        return float(np.mean([e[i].elapsed_time(e[j]) for e in evs]))
+    kern = {"state": mean(0, 1), "grad": mean(1, 2), "node_flux": mean(2, 3),
+            "surface": mean(3, 4), "rhs": mean(2, 4)}
     return float(np.sum(step_ms)), kern
 
 
@@ -450,25 +500,28 @@ def run_ours(args):
     hbm, peak_kind = _peaks()
     ab = algorithmic_bytes(dcoll, nc, s=4, mixture=mixture)
     k32 = res[head][1]
-    kt = {k: v for k, v in k32.items() if k in ab}
+    kt = {k: v for k, v in k32.items() if k in ab and k != "rhs"}
     top = max(kt, key=kt.get)
     achieved = ab[top] / (kt[top] / 1e3) / 1e9
     ab64 = algorithmic_bytes(dcoll, nc, s=8, mixture=mixture)
     k64 = res["plain_fp64"][1]
-    kt64 = {k: v for k, v in k64.items() if k in ab64}
+    kt64 = {k: v for k, v in k64.items() if k in ab64 and k != "rhs"}
     top64 = max(kt64, key=kt64.get)
-    traffic = None
+    traffic = traffic64 = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(args.workload, {}).get("mixed_" + top)
+            tj = json.load(f).get(args.workload, {})
+        traffic = tj.get("mixed_" + top)
+        traffic64 = tj.get("plain_fp64_" + top64)
 
     if rank != 0:
         return
     cpu = cpu_baseline(args.workload) if world == 1 and not args.no_cpu else None
-    launches_per_step = {"plain_fp64": 3 if mixture else 2,
-                         "mixed_plain_guess": 3 if mixture else 2,
-                         "mixed_learned": 4}
+    # this library's kernels per step: temperature (mixtures), gradient, and
+    # the divergence pass (node flux + surface on the split path)
+    from mirgecom_b200 import runtime as _rt
+    per_step = (1 if mixture else 0) + 1 + (2 if _rt.SPLIT_RHS else 1)
     line = {
         "metric": "DOF-RHS evals/s", "value": values[head], "unit": "DOF-RHS/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -488,12 +541,17 @@ def run_ours(args):
         "learned_guess": learned,
         "e2e": {"value": e2e_value, "unit": "DOF-RHS/s",
                 "h2d_bytes_per_step": hq.numel() * 4, "d2h_bytes_per_step": hq.numel() * 4},
-        "gpu_launches": sum(launches_per_step[n] for n in names) * args.steps,
-        "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm,
+        "gpu_launches": per_step * args.steps,
+        "gpu_launches_note": "headline form's timed steps; each form launches the same "
+                             f"{per_step} kernels per step",
+        "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES.get(top, top), "phase": top,
+                     "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                      "algorithmic_bytes": ab[top], "traffic": traffic},
-        "roofline_plain_fp64": {"kernel": top64,
-                                "frac": ab64[top64] / (kt64[top64] / 1e3) / 1e9 / hbm},
+        "roofline_plain_fp64": {"kernel": KERNEL_NAMES.get(top64, top64), "phase": top64,
+                                "achieved": ab64[top64] / (kt64[top64] / 1e3) / 1e9,
+                                "frac": ab64[top64] / (kt64[top64] / 1e3) / 1e9 / hbm,
+                                "algorithmic_bytes": ab64[top64], "traffic": traffic64},
         "device_status": status,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),

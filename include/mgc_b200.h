@@ -204,17 +204,21 @@ int mgc_rk4_stage_mixed(int64_t n, const double* q0, const float* k, double* sum
  * workspace, then the numerical face fluxes from the records of both sides
  * and the tensor-core contraction.  Same arguments and results as the fused
  * entry points plus the workspace (16-byte aligned, at least
- * mgc_rhs_split_workspace_bytes(mesh, gas, single_precision) bytes). ---- */
+ * mgc_rhs_split_workspace_bytes(mesh, gas, single_precision) bytes) and
+ * mid_event, a cudaEvent_t recorded on the stream between the two kernels
+ * (NULL for none; for timing the surface kernel on its own). ---- */
 size_t mgc_rhs_split_workspace_bytes(const mgc_mesh_t* mesh, const mgc_gas_t* gas,
                                      int single_precision);
 int mgc_rhs_split(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
                   const double* t_op, const double* t_src, const double* grad,
                   const double* bext, int flux_kind, int add_sources, double* rhs,
-                  void* workspace, size_t workspace_bytes, int32_t* status, void* stream);
+                  void* workspace, size_t workspace_bytes, int32_t* status, void* stream,
+                  void* mid_event);
 int mgc_rhs_split_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
                       const float* t_op, const float* t_src, const float* grad,
                       const float* bext, int flux_kind, int add_sources, float* rhs,
-                      void* workspace, size_t workspace_bytes, int32_t* status, void* stream);
+                      void* workspace, size_t workspace_bytes, int32_t* status, void* stream,
+                      void* mid_event);
 
 /* ---- learned initial guess of the mixture temperature (no counterpart in
  * the reference, whose Newton solve always starts from the seed): an

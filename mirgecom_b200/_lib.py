@@ -97,9 +97,9 @@ _SIGNATURES = {
     "mgc_rk4_stage_mixed": ([C.c_int64, _P, _P, _P, _P, _P, C.c_int, C.c_double, _P], C.c_int),
     "mgc_rhs_split_workspace_bytes": ([_P, _P, C.c_int], C.c_size_t),
     "mgc_rhs_split": ([C.c_int, _P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P,
-                       C.c_size_t, _P, _P], C.c_int),
+                       C.c_size_t, _P, _P, _P], C.c_int),
     "mgc_rhs_split_f32": ([C.c_int, _P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P,
-                           C.c_size_t, _P, _P], C.c_int),
+                           C.c_size_t, _P, _P, _P], C.c_int),
     "mgc_mlp_nparams": ([], C.c_int),
     "mgc_mlp_refresh": ([_P, _P], C.c_int),
     "mgc_mlp_infer": ([C.c_int, C.c_int, C.c_int64, _P, _P, _P, _P], C.c_int),

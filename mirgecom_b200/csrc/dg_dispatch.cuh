@@ -131,6 +131,8 @@ struct Launch {
     if (nb > 148 * 64) nb = 148 * 64;
     k_node_flux<R, DIM, ORDER, NS, MIX, VISC><<<(unsigned)nb, 128, 0, s>>>(a, g);
     if (cudaGetLastError() != cudaSuccess) return MGC_E_CUDA;
+    if (a.mid_event && cudaEventRecord(static_cast<cudaEvent_t>(a.mid_event), s) != cudaSuccess)
+      return MGC_E_CUDA;
     const size_t smem = C::smem_surface(a.nperm);
     auto kern = k_surface<R, DIM, ORDER, NS, MIX, VISC>;
     int rc = prepare_kernel(kern, smem);

@@ -54,6 +54,8 @@ struct DGArgs {
   int32_t pad_;
   R* fbuf;             // split path: per-node flux record [E*NP][FW]
   R* srcbuf;           // split path: species sources [NS][E][NP]
+  void* mid_event;     // split path (host side): cudaEvent_t recorded between
+                       // the node-flux and surface kernels, or null
 };
 
 enum BoundaryKind { BK_DUMMY = 0, BK_PRESCRIBED = 1 };

@@ -177,7 +177,7 @@ template <class R>
 int rhs_split_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const R* q,
                    const R* t_op, const R* t_src, const R* grad, const R* bext, int flux_kind,
                    int add_sources, R* rhs, void* workspace, size_t workspace_bytes,
-                   int32_t* status, void* stream) {
+                   int32_t* status, void* stream, void* mid_event) {
   if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !rhs || !status || !workspace)
     return MGC_E_INVALID;
   if (visc && !grad) return MGC_E_INVALID;
@@ -193,6 +193,7 @@ int rhs_split_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const
   DGArgs<R> a = make_args<R>(mesh, q, t_op, t_src, grad, rhs, bext, flux_kind, add_sources,
                              status);
   a.fbuf = static_cast<R*>(workspace);
+  a.mid_event = mid_event;
   // sources after the flux records, 16-byte aligned
   const size_t rec_bytes = need - 256 - (size_t)gas->nspecies * mesh->nelem *
                                             mgc::simplex_npts(mesh->dim, mesh->order) * sizeof(R);
@@ -213,17 +214,21 @@ size_t mgc_rhs_split_workspace_bytes(const mgc_mesh_t* mesh, const mgc_gas_t* ga
 int mgc_rhs_split(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
                   const double* t_op, const double* t_src, const double* grad,
                   const double* bext, int flux_kind, int add_sources, double* rhs,
-                  void* workspace, size_t workspace_bytes, int32_t* status, void* stream) {
+                  void* workspace, size_t workspace_bytes, int32_t* status, void* stream,
+                  void* mid_event) {
   return rhs_split_impl<double>(viscous, mesh, gas, q, t_op, t_src, grad, bext, flux_kind,
-                                add_sources, rhs, workspace, workspace_bytes, status, stream);
+                                add_sources, rhs, workspace, workspace_bytes, status, stream,
+                                mid_event);
 }
 
 int mgc_rhs_split_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
                       const float* t_op, const float* t_src, const float* grad,
                       const float* bext, int flux_kind, int add_sources, float* rhs,
-                      void* workspace, size_t workspace_bytes, int32_t* status, void* stream) {
+                      void* workspace, size_t workspace_bytes, int32_t* status, void* stream,
+                      void* mid_event) {
   return rhs_split_impl<float>(viscous, mesh, gas, q, t_op, t_src, grad, bext, flux_kind,
-                               add_sources, rhs, workspace, workspace_bytes, status, stream);
+                               add_sources, rhs, workspace, workspace_bytes, status, stream,
+                               mid_event);
 }
 
 

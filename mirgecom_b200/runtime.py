@@ -253,7 +253,7 @@ def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
             _lib.check(fsplit(0, C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op),
                               None, None, _lib.ptr(bext), flux_kind, 0, _lib.ptr(rhs),
                               _lib.ptr(ws), ws.numel(), _lib.ptr(dd.status),
-                              _lib.stream_handle()), "mgc_rhs_split")
+                              _lib.stream_handle(), None), "mgc_rhs_split")
         return rhs
     fn = lib.mgc_euler_rhs_f32 if f32 else lib.mgc_euler_rhs
     with torch.cuda.device(q.device):
@@ -266,8 +266,10 @@ def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
 
 def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
            source_temperature=None, grad_out=None, events=None):
-    """Gradient + divergence passes.  *events* (3 CUDA events) are recorded
-    before the gradient pass, between the passes and after the divergence."""
+    """Gradient + divergence passes.  *events* (3 or 4 CUDA events) are
+    recorded before the gradient pass, between the passes, (with 4: between
+    the node-flux and surface kernels of the split divergence) and after the
+    divergence."""
     q = state.cv.q
     _lib.require_cuda(q)
     q = q.contiguous()
@@ -301,17 +303,23 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
         if SPLIT_RHS:
             ws = _split_workspace(dd, gs, f32)
             fsplit = lib.mgc_rhs_split_f32 if f32 else lib.mgc_rhs_split
+            mid = None
+            if events and len(events) == 4:
+                # the event exists once recorded; the library records it
+                # again between its two kernels
+                events[2].record()
+                mid = events[2].cuda_event
             _lib.check(fsplit(1, C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op),
                               _lib.ptr(t_src), _lib.ptr(grad), _lib.ptr(bext), flux_kind,
                               int(add_src), _lib.ptr(rhs), _lib.ptr(ws), ws.numel(),
-                              _lib.ptr(dd.status), stream), "mgc_rhs_split")
+                              _lib.ptr(dd.status), stream, mid), "mgc_rhs_split")
         else:
             _lib.check(frhs(
                 C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(t_src),
                 _lib.ptr(grad), _lib.ptr(bext), flux_kind, int(add_src), _lib.ptr(rhs),
                 _lib.ptr(dd.status), stream), "mgc_ns_rhs")
         if events:
-            events[2].record()
+            events[-1].record()
     return rhs, grad
 
 
