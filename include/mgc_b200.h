@@ -56,6 +56,8 @@ extern "C" {
 #define MGC_FLUX_RUSANOV 0
 #define MGC_FLUX_HLL 1
 #define MGC_FLUX_CENTRAL 2
+#define MGC_ELEM_SIMPLEX 0
+#define MGC_ELEM_HEX 1       /* tensor-product (GLL) hexahedra, affine */
 
 /* Gas model: GasModel(eos, transport), mirgecom/gas_model.py:82-97, with
  * IdealSingleGas (mirgecom/eos.py:302), PyrometheusMixture (eos.py:540),
@@ -96,7 +98,8 @@ typedef struct {
 /* Flattened discretization (the host-side replacement of grudge's
  * DiscretizationCollection connectivity, mirgecom/discretization.py:41-83). */
 typedef struct {
-  int32_t dim, order, nelem, nbf, nperm, pad_;
+  int32_t dim, order, nelem, nbf, nperm;
+  int32_t elem_kind;        /* MGC_ELEM_SIMPLEX or MGC_ELEM_HEX */
   const double* rx;
   const int32_t* conn;
   const uint8_t* perm;
@@ -119,6 +122,18 @@ int mgc_upload_reference_operators(int dim, int order, const double* weak_host,
                                    const double* ref_normals_host,
                                    const double* face_scale_ref_host,
                                    const int32_t* face_nodes_host);
+
+/* Tensor-product hexahedra (TensorProductElementGroup meshes,
+ * mirgecom/discretization.py:41-83 with tensor-product groups; the operators
+ * of operators.py:34-95 applied by sum factorisation).  Upload the 1-D
+ * operators of order p: weak1d [p+1][p+1] = M1^-1 D1^T M1, lift1d [p+1][2] =
+ * columns 0 and p of M1^-1, and the reference face scale.  Supported: dim 3,
+ * p = 1..4, single ideal gas; the gradient pass (mgc_ns_grad*) and the split
+ * divergence (mgc_rhs_split*) -- the fused mgc_euler_rhs / mgc_ns_rhs return
+ * MGC_E_UNSUPPORTED for hexahedra. */
+int mgc_supports_hex(int dim, int order, int nspecies, int eos_kind);
+int mgc_upload_hex_operators(int dim, int order, const double* weak1d_host,
+                             const double* lift1d_host, double face_scale_ref);
 
 /* Upload a thermochemistry mechanism (pyrometheus class data used by
  * PyrometheusMixture, mirgecom/eos.py:540-888) on the current device. */

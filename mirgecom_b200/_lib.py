@@ -61,7 +61,7 @@ class MechanismStruct(C.Structure):
 class MeshStruct(C.Structure):
     _fields_ = [
         ("dim", C.c_int32), ("order", C.c_int32), ("nelem", C.c_int32),
-        ("nbf", C.c_int32), ("nperm", C.c_int32), ("pad_", C.c_int32),
+        ("nbf", C.c_int32), ("nperm", C.c_int32), ("elem_kind", C.c_int32),
         ("rx", C.c_void_p), ("conn", C.c_void_p), ("perm", C.c_void_p),
         ("bkind", C.c_void_p), ("rx32", C.c_void_p),
     ]
@@ -82,6 +82,8 @@ _SIGNATURES = {
     "mgc_upload_reference_operators": (
         [C.c_int, C.c_int, _P, _P, _P, _P, _P], C.c_int),
     "mgc_set_mechanism": ([_P], C.c_int),
+    "mgc_supports_hex": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+    "mgc_upload_hex_operators": ([C.c_int, C.c_int, _P, _P, C.c_double], C.c_int),
     "mgc_mixture_temperature": ([C.c_int, _P, C.c_int64, _P, _P, _P, _P, _P], C.c_int),
     "mgc_euler_rhs": ([_P, _P, _P, _P, _P, C.c_int, _P, _P, _P], C.c_int),
     "mgc_ns_grad": ([_P, _P, _P, _P, _P, _P, _P, _P], C.c_int),

@@ -129,7 +129,7 @@ struct Launch {
     const int64_t nn = (int64_t)a.nelem * C::NP;
     int64_t nb = (nn + 127) / 128;
     if (nb > 148 * 64) nb = 148 * 64;
-    k_node_flux<R, DIM, ORDER, NS, MIX, VISC><<<(unsigned)nb, 128, 0, s>>>(a, g);
+    k_node_flux<R, DIM, C::NP, NS, MIX, VISC><<<(unsigned)nb, 128, 0, s>>>(a, g);
     if (cudaGetLastError() != cudaSuccess) return MGC_E_CUDA;
     if (a.mid_event && cudaEventRecord(static_cast<cudaEvent_t>(a.mid_event), s) != cudaSuccess)
       return MGC_E_CUDA;

@@ -858,11 +858,19 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
 // The split trades one record write + read per node for the 2-3x repeated
 // neighbour-state evaluations of the fused kernel.
 
-template <class R, int DIM, int ORDER, int NS, bool MIX, bool VISC>
-__global__ void __launch_bounds__(128, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_NODE))
+// Flux record width: NC*DIM total-flux values, then p, c, gamma, padded to 16 bytes.
+__host__ __device__ constexpr int flux_record_width(int dim, int nc) {
+  return round_up(nc * dim + 3, 4);
+}
+
+// resident 128-thread blocks of the node-flux kernel: the float64 mixture
+// state needs more registers per thread
+__host__ __device__ constexpr int node_flux_minb(int rb, int ns) { return (rb == 8 && ns > 2) ? 3 : 4; }
+
+template <class R, int DIM, int NP, int NS, bool MIX, bool VISC>
+__global__ void __launch_bounds__(128, node_flux_minb((int)sizeof(R), NS))
     k_node_flux(DGArgs<R> a, GasParams g) {
-  using C = Cfg<R, DIM, ORDER, NS, MIX>;
-  constexpr int NP = C::NP, NC = C::NC, FW = C::FW;
+  constexpr int NC = DIM + 2 + NS, FW = flux_record_width(DIM, NC);
   const int64_t EN = (int64_t)a.nelem * NP;
   const bool sources = MIX && a.add_sources;
   bool bad = false;
@@ -985,14 +993,13 @@ __device__ __forceinline__ void load_group(const R* __restrict__ src, int v0, in
 // field c to bcol[c * cstride].  Out of line (arguments by value, no
 // address of a caller variable taken), so that its face states do not enter
 // the register allocation of the interior fast path.
-template <class R, int DIM, int ORDER, int NS, bool MIX, bool VISC>
+template <class R, int DIM, int NP, int NFP, int NS, bool MIX, bool VISC>
 __device__ __noinline__ void surface_face_general(const DGArgs<R> a, const GasParams g,
                                                   int64_t EN, int64_t gm, int64_t g0, int m,
                                                   int cn, R n0, R n1, R n2, R fsc,
                                                   const uint8_t* perm_s, R* bcol, int cstride) {
   const R n[3] = {n0, n1, n2};
-  using C = Cfg<R, DIM, ORDER, NS, MIX>;
-  constexpr int NP = C::NP, NFP = C::NFP, NC = C::NC, FW = C::FW;
+  constexpr int NC = DIM + 2 + NS, FW = flux_record_width(DIM, NC);
   const int E = a.nelem;
   R fr[FW], f0[FW];
   load_record<R, FW>(a.fbuf + gm * FW, fr);
@@ -1242,7 +1249,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
           bcol[c * EPB * KB] = fsc * (out - s0);
         }
       } else if (grp == 0) {
-        surface_face_general<R, DIM, ORDER, NS, MIX, VISC>(
+        surface_face_general<R, DIM, NP, NFP, NS, MIX, VISC>(
             a, g, EN, gm, g0, m, cn, n[0], n[1], DIM > 2 ? n[DIM - 1] : R(0), fsc, perm_s,
             bcol, EPB * KB);
       }

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "dg_dispatch.cuh"
+#include "hex_kernels.cuh"
 
 namespace mgc {
 int tu2_upload_refops(int, int, const double*, const float*, const int*);
@@ -32,6 +33,12 @@ size_t tu2_split_workspace(int, int, bool, int64_t);
 size_t tu3_split_workspace(int, int, bool, int64_t);
 size_t tu2f_split_workspace(int, int, bool, int64_t);
 size_t tu3f_split_workspace(int, int, bool, int64_t);
+int tuh_upload_hexops(const double*);
+int tuhf_upload_hexops(const double*);
+int tuh_dispatch(int, int, int, bool, const DGArgs<double>&, const GasParams&, cudaStream_t);
+int tuhf_dispatch(int, int, int, bool, const DGArgs<float>&, const GasParams&, cudaStream_t);
+size_t tuh_split_workspace(int, int, bool, int64_t);
+size_t tuhf_split_workspace(int, int, bool, int64_t);
 }  // namespace mgc
 
 using namespace mgc;
@@ -41,7 +48,20 @@ namespace {
 // per-device record of which reference operators / mechanism were uploaded
 constexpr int kMaxDevices = 64;
 bool g_refops_ready[kMaxDevices][8] = {};
+bool g_hexops_ready[kMaxDevices][8] = {};
 bool g_mech_ready[kMaxDevices] = {};
+
+// 1-D operators of the tensor-product hexahedra uploaded so far (host copy
+// of the packed constant block; each upload adds one order)
+constexpr int kHexPacked = 200;
+double g_hexops_host[kHexPacked] = {};
+
+constexpr int kElemSimplex = 0, kElemHex = 1;
+
+int mesh_npts(const mgc_mesh_t* m) {
+  return m->elem_kind == kElemHex ? (m->order + 1) * (m->order + 1) * (m->order + 1)
+                                  : simplex_npts(m->dim, m->order);
+}
 
 int current_device() {
   int d = 0;
@@ -51,6 +71,7 @@ int current_device() {
 
 bool mesh_ok(const mgc_mesh_t* m) {
   return m && (m->dim == 2 || m->dim == 3) && m->nelem > 0 && m->rx && m->conn &&
+         (m->elem_kind == kElemSimplex || (m->elem_kind == kElemHex && m->dim == 3)) &&
          m->nperm > 0 && m->nperm <= 256 && m->perm && m->nbf >= 0 &&
          (m->nbf == 0 || m->bkind) && (int64_t)m->nelem * 256 < (int64_t)1 << 31;
 }
@@ -63,9 +84,14 @@ bool gas_ok(const mgc_gas_t* g) {
 int ready(const mgc_mesh_t* m, const mgc_gas_t* g) {
   const int dev = current_device();
   if (dev < 0) return MGC_E_CUDA;
-  const int slot = refops_slot(m->dim, m->order);
-  if (slot < 0) return MGC_E_UNSUPPORTED;
-  if (!g_refops_ready[dev][slot]) return MGC_E_NOT_READY;
+  if (m->elem_kind == kElemHex) {
+    if (m->order < 1 || m->order > kHexMaxOrder) return MGC_E_UNSUPPORTED;
+    if (!g_hexops_ready[dev][m->order]) return MGC_E_NOT_READY;
+  } else {
+    const int slot = refops_slot(m->dim, m->order);
+    if (slot < 0) return MGC_E_UNSUPPORTED;
+    if (!g_refops_ready[dev][slot]) return MGC_E_NOT_READY;
+  }
   if (g->eos_kind == MGC_EOS_MIXTURE && !g_mech_ready[dev]) return MGC_E_NOT_READY;
   return MGC_OK;
 }
@@ -110,6 +136,7 @@ int dispatch(int op, const mgc_mesh_t* m, const mgc_gas_t* g, const DGArgs<doubl
   const bool mix = g->eos_kind == MGC_EOS_MIXTURE;
   if (!supported_species(g->nspecies, mix)) return MGC_E_UNSUPPORTED;
   const GasParams p = to_params(g);
+  if (m->elem_kind == kElemHex) return tuh_dispatch(op, m->order, g->nspecies, mix, a, p, s);
   if (m->dim == 2) return tu2_dispatch(op, m->order, g->nspecies, mix, a, p, s);
   return tu3_dispatch(op, m->order, g->nspecies, mix, a, p, s);
 }
@@ -120,6 +147,7 @@ int dispatch(int op, const mgc_mesh_t* m, const mgc_gas_t* g, const DGArgs<float
   if (!supported_species_f32(g->nspecies, mix)) return MGC_E_UNSUPPORTED;
   if (!m->rx32) return MGC_E_INVALID;
   const GasParams p = to_params(g);
+  if (m->elem_kind == kElemHex) return tuhf_dispatch(op, m->order, g->nspecies, mix, a, p, s);
   if (m->dim == 2) return tu2f_dispatch(op, m->order, g->nspecies, mix, a, p, s);
   return tu3f_dispatch(op, m->order, g->nspecies, mix, a, p, s);
 }
@@ -166,6 +194,9 @@ int ns_rhs_impl(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const R* q, const 
 template <class R>
 size_t split_ws(const mgc_mesh_t* m, const mgc_gas_t* g) {
   const bool mix = g->eos_kind == MGC_EOS_MIXTURE;
+  if (m->elem_kind == kElemHex)
+    return sizeof(R) == 8 ? tuh_split_workspace(m->order, g->nspecies, mix, m->nelem)
+                          : tuhf_split_workspace(m->order, g->nspecies, mix, m->nelem);
   if constexpr (sizeof(R) == 8)
     return m->dim == 2 ? tu2_split_workspace(m->order, g->nspecies, mix, m->nelem)
                        : tu3_split_workspace(m->order, g->nspecies, mix, m->nelem);
@@ -195,8 +226,8 @@ int rhs_split_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const
   a.fbuf = static_cast<R*>(workspace);
   a.mid_event = mid_event;
   // sources after the flux records, 16-byte aligned
-  const size_t rec_bytes = need - 256 - (size_t)gas->nspecies * mesh->nelem *
-                                            mgc::simplex_npts(mesh->dim, mesh->order) * sizeof(R);
+  const size_t rec_bytes =
+      need - 256 - (size_t)gas->nspecies * mesh->nelem * mesh_npts(mesh) * sizeof(R);
   a.srcbuf = reinterpret_cast<R*>(static_cast<char*>(workspace) + ((rec_bytes + 15) / 16) * 16);
   return dispatch(visc ? 4 : 3, mesh, gas, a, (cudaStream_t)stream);
 }
@@ -237,6 +268,31 @@ int mgc_version(void) { return 1; }
 int mgc_supports(int dim, int order, int nspecies, int eos_kind) {
   if (refops_slot(dim, order) < 0) return 0;
   return supported_species(nspecies, eos_kind == MGC_EOS_MIXTURE) ? 1 : 0;
+}
+
+int mgc_supports_hex(int dim, int order, int nspecies, int eos_kind) {
+  return (dim == 3 && order >= 1 && order <= kHexMaxOrder && nspecies == 0 &&
+          eos_kind == MGC_EOS_IDEAL) ? 1 : 0;
+}
+
+int mgc_upload_hex_operators(int dim, int order, const double* weak1d_host,
+                             const double* lift1d_host, double face_scale_ref) {
+  if (dim != 3 || order < 1 || order > kHexMaxOrder) return MGC_E_UNSUPPORTED;
+  if (!weak1d_host || !lift1d_host || !(face_scale_ref > 0.0)) return MGC_E_INVALID;
+  static_assert(kHexOpsTotal <= kHexPacked, "hex operator block");
+  const int n1 = order + 1;
+  double* p = g_hexops_host + hexops_offset(order);
+  for (int i = 0; i < n1 * n1; ++i) p[i] = weak1d_host[i];
+  for (int i = 0; i < 2 * n1; ++i) p[n1 * n1 + i] = lift1d_host[i];
+  p[n1 * n1 + 2 * n1] = face_scale_ref;
+  int rc = tuh_upload_hexops(g_hexops_host);
+  if (rc) return rc;
+  rc = tuhf_upload_hexops(g_hexops_host);
+  if (rc) return rc;
+  const int dev = current_device();
+  if (dev < 0) return MGC_E_CUDA;
+  g_hexops_ready[dev][order] = true;
+  return MGC_OK;
 }
 
 int mgc_upload_reference_operators(int dim, int order, const double* weak_host,

@@ -64,6 +64,8 @@ int mgc_ns_operator_noalloc(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const 
   if (!mesh || !gas || mesh->nelem <= 0 || gas->nspecies < 0 ||
       (mesh->dim != 2 && mesh->dim != 3) || mesh->order < 1)
     return MGC_E_INVALID;
+  // simplicial meshes only: hexahedra have no fused divergence pass
+  if (mesh->elem_kind != MGC_ELEM_SIMPLEX) return MGC_E_UNSUPPORTED;
   const size_t np = (size_t)mgc::simplex_npts(mesh->dim, mesh->order);
   const size_t nc = (size_t)(mesh->dim + 2 + gas->nspecies);
   const size_t need = (nc + 1) * (size_t)mesh->dim * (size_t)mesh->nelem * np;

@@ -15,7 +15,7 @@ import torch
 
 from mirgecom_b200 import _lib
 
-_uploaded_refops = set()     # (device index, dim, order)
+_uploaded_refops = set()     # (device index, element kind, dim, order)
 _uploaded_mech = {}          # device index -> id(mechanism)
 
 
@@ -24,13 +24,23 @@ def _dev_index(device):
 
 
 def ensure_reference_operators(dcoll, device):
-    key = (_dev_index(device), dcoll.dim, dcoll.order)
+    key = (_dev_index(device), dcoll.refel.kind, dcoll.dim, dcoll.order)
     if key in _uploaded_refops:
         return
     r = dcoll.refel
-    if r.kind != "simplex":
-        raise NotImplementedError("device kernels cover simplicial elements")
     lib = _lib.load()
+    if r.kind == "hypercube":
+        if not lib.mgc_supports_hex(dcoll.dim, dcoll.order, 0, _lib.EOS_IDEAL):
+            raise NotImplementedError(
+                f"no device kernels for {dcoll.dim}-D hexahedra of order {dcoll.order}")
+        w1 = np.ascontiguousarray(r.extra["weak1d"], dtype=np.float64)
+        l1 = np.ascontiguousarray(r.extra["mass1d_inv"][:, [0, -1]], dtype=np.float64)
+        with torch.cuda.device(device):
+            _lib.check(lib.mgc_upload_hex_operators(
+                dcoll.dim, dcoll.order, _lib.ptr(w1), _lib.ptr(l1),
+                float(r.face_scale_ref[0])), "mgc_upload_hex_operators")
+        _uploaded_refops.add(key)
+        return
     arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
             (r.weak, r.lift, r.ref_face_normals, r.face_scale_ref)]
     fn = np.ascontiguousarray(r.face_nodes, dtype=np.int32)
@@ -81,6 +91,7 @@ class DeviceDiscretization:
         self.mesh.perm = self.perm.data_ptr()
         self.mesh.bkind = None
         self.mesh.rx32 = self.rx32.data_ptr()
+        self.mesh.elem_kind = 1 if dcoll.refel.kind == "hypercube" else 0
 
     def workspace(self, name, shape, dtype=torch.float64):
         t = self._work.get(name)

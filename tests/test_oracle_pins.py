@@ -29,12 +29,15 @@ def _uniform_q(dim, nspecies, shape):
     return q
 
 
-@pytest.mark.parametrize("dim,order", [(2, 1), (2, 3), (3, 1), (3, 2)])
+@pytest.mark.parametrize("kind,dim,order", [("simplex", 2, 1), ("simplex", 2, 3),
+                                            ("simplex", 3, 1), ("simplex", 3, 2),
+                                            ("hypercube", 2, 3), ("hypercube", 3, 2)])
 @pytest.mark.parametrize("nspecies", [0, 3])
 @pytest.mark.parametrize("flux", ["rusanov", "hll"])
-def test_uniform_state_euler_rhs_vanishes(dim, order, nspecies, flux):
-    """test/test_euler.py:87-236: a uniform state gives rhs = 0 to FP."""
-    _, od = make_disc("simplex", dim, 3, order, (-0.5,) * dim, (0.5,) * dim, True)
+def test_uniform_state_euler_rhs_vanishes(kind, dim, order, nspecies, flux):
+    """test/test_euler.py:87-236 (tpe True and False): a uniform state gives
+    rhs = 0 to FP."""
+    _, od = make_disc(kind, dim, 3, order, (-0.5,) * dim, (0.5,) * dim, True)
     q = _uniform_q(dim, nspecies, od.nodes.shape[1:])
     gas = oph.IdealGas()
     st = oph.make_fluid_state(q, gas, None, dim)
@@ -42,10 +45,11 @@ def test_uniform_state_euler_rhs_vanishes(dim, order, nspecies, flux):
     assert np.abs(rhs).max() < 1e-9
 
 
-@pytest.mark.parametrize("dim,order", [(2, 2), (3, 1)])
-def test_uniform_state_ns_rhs_vanishes(dim, order):
+@pytest.mark.parametrize("kind,dim,order", [("simplex", 2, 2), ("simplex", 3, 1),
+                                            ("hypercube", 3, 4)])
+def test_uniform_state_ns_rhs_vanishes(kind, dim, order):
     """test/test_navierstokes.py:86-225: uniform state, viscous terms on."""
-    _, od = make_disc("simplex", dim, 3, order, (-0.5,) * dim, (0.5,) * dim, True)
+    _, od = make_disc(kind, dim, 3, order, (-0.5,) * dim, (0.5,) * dim, True)
     q = _uniform_q(dim, 2, od.nodes.shape[1:])
     gas = oph.IdealGas()
     tr = oph.SimpleTransportParams(viscosity=1e-2, thermal_conductivity=1e-2,
@@ -59,13 +63,15 @@ def _eoc(hs, errs):
     return float(np.polyfit(np.log(hs), np.log(errs), 1)[0])
 
 
-@pytest.mark.parametrize("order", [1, 2, 3])
-def test_static_vortex_rhs_converges(order):
-    """test/test_euler.py:410-485: the static isentropic vortex is a steady
-    solution, so rhs -> 0 at order >= p - 0.7 with exact boundary states."""
+@pytest.mark.parametrize("kind,order", [("simplex", 1), ("simplex", 2), ("simplex", 3),
+                                        ("hypercube", 2), ("hypercube", 3)])
+def test_static_vortex_rhs_converges(kind, order):
+    """test/test_euler.py:410-485 (tpe True and False): the static isentropic
+    vortex is a steady solution, so rhs -> 0 at order >= p - 0.7 with exact
+    boundary states."""
     hs, errs = [], []
     for n in (24, 32, 48):
-        _, od = make_disc("simplex", 2, n, order, (-5.0, -5.0), (5.0, 5.0), False)
+        _, od = make_disc(kind, 2, n, order, (-5.0, -5.0), (5.0, 5.0), False)
         q = vortex_np(od.nodes, center=(0.0, 0.0), vel=(0.0, 0.0))
         gas = oph.IdealGas()
         st = oph.make_fluid_state(q, gas, None, 2)
