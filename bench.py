@@ -66,6 +66,12 @@ WORKLOADS = {
              "order 3 (20 nodes/tet, 3.9M nodes): the reacting_p3_tet80 physics with inputs "
              "larger than L2 and a few GB on the device, for kernel captures",
         n=32, order=3, kind="reacting"),
+    "tgv_p4_hex48": dict(
+        desc="3-D viscous Taylor-Green vortex, periodic [-pi,pi]^3, 48^3 tensor-product "
+             "hexahedra (110,592), order 4 (125 nodes/element, 13.8M nodes), ideal gas "
+             "gamma=1.4, Mach 0.1, Re 1600, Pr 0.71, Rusanov + BR1; sum-factorised "
+             "contractions",
+        n=48, order=4, kind="tgv", elem="hypercube"),
     "tgv_p3_tet24": dict(
         desc="3-D viscous Taylor-Green vortex, periodic [-pi,pi]^3, 24^3 hexes x 6 tets "
              "(82,944 tets), order 3 (20 nodes/tet), ideal gas gamma=1.4, Mach 0.1, "
@@ -87,12 +93,13 @@ def build_workload(name, device):
     from mirgecom_b200.thermochemistry import UIUC_7SP
     from mirgecom_b200.transport import SimpleTransport
     w = WORKLOADS[name]
+    elem = w.get("elem", "simplex")
     if w["kind"] == "tgv":
         mesh = generate_box_mesh((-np.pi,) * 3, (np.pi,) * 3, (w["n"],) * 3,
-                                 periodic=(True,) * 3)
+                                 kind=elem, periodic=(True,) * 3)
     else:
         mesh = generate_box_mesh((0.0,) * 3, (2 * np.pi,) * 3, (w["n"],) * 3,
-                                 periodic=(True,) * 3)
+                                 kind=elem, periodic=(True,) * 3)
     dcoll = Discretization(mesh, w["order"], device=device)
     x = [t for t in dcoll.nodes(device)]
     if w["kind"] == "tgv":
@@ -216,7 +223,7 @@ def _oracle_setup(name):
     if w["kind"] == "tgv":
         n_sample = 6
         mesh = generate_box_mesh((-np.pi,) * 3, (np.pi,) * 3, (n_sample,) * 3,
-                                 periodic=(True,) * 3)
+                                 kind=w.get("elem", "simplex"), periodic=(True,) * 3)
         mu = 1 / 1600
         otr = oph.SimpleTransportParams(viscosity=mu, thermal_conductivity=mu * 1004.85 / 0.71)
         gas = oph.IdealGas()
@@ -280,7 +287,8 @@ def cpu_baseline(name, seconds=10.0):
     q, tseed = _oracle_state(name, od)
     value, reps, nel, n_sample = _time_oracle(name, q, tseed, seconds)
     return {"value": value, "unit": "DOF-RHS/s", "cores": 1, "kind": "port",
-            "sample": f"{n_sample}^3 x 6 tets ({nel} tets, {q.size} DOF), same physics and "
+            "sample": f"{n_sample}^3 mesh ({nel} elements, {q.size} DOF), same physics, "
+                      f"element and "
                       f"order as {name}, {reps} RHS evaluations, numpy float64 oracle, "
                       f"one process"}
 
@@ -311,8 +319,8 @@ def run_reference(args):
     value = float(sum(r[0] for r in res))
     reps = sum(r[1] for r in res)
     _, _, nel, n_sample = res[0]
-    sample = (f"{n_sample}^3 x 6 tets ({nel} tets, {q.size} DOF), same physics and order "
-              f"as {args.workload}, {reps} RHS evaluations over {ncores} processes, numpy "
+    sample = (f"{n_sample}^3 mesh ({nel} elements, {q.size} DOF), same physics, element "
+              f"and order as {args.workload}, {reps} RHS evaluations over {ncores} processes, numpy "
               f"float64 oracle (the reference's CPU path restated; its runtime is not "
               f"installed)")
     line = {"impl": "reference", "metric": "DOF-RHS evals/s", "value": value,
@@ -399,6 +407,50 @@ def _train_guess(dev, seed=0, steps=2000, samples=1 << 20):
                  "loss_first": hist[0], "loss_final": hist[-1], "heldout_rms_K": rms}
 
 
+def _end_of_run(dcoll, gas, q64, nsteps, n_axis):
+    """*nsteps* RK4 steps of the float64 form and of the mixed form (float64
+    RK accumulation, float32 right-hand sides) from the same state: the
+    per-field relative L2 difference at the end, next to how far the state
+    moved.  The float64 device path stands in for the oracle at this size (it
+    matches the oracle to 1e-12 in the parity tests)."""
+    import torch
+
+    from mirgecom_b200.fluid import ConservedVars
+    from mirgecom_b200.gas_model import make_fluid_state
+    from mirgecom_b200.integrators import rk4_step, rk4_step_mixed
+    from mirgecom_b200.navierstokes import ns_operator
+    h = 2 * np.pi / n_axis
+    p = dcoll.order
+    # acoustic CFL 0.3 with the (p+1)^2 DG scaling: |u| + c <= 11 at Mach 0.1
+    dt = 0.3 * h / (p + 1) ** 2 / 11.0
+
+    def rhs(t, cv):
+        return ns_operator(dcoll, gas, make_fluid_state(cv, gas), {})
+
+    s64 = ConservedVars(q64.clone(), 3)
+    shi = ConservedVars(q64.clone(), 3)
+    slo = None
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(nsteps):
+        s64 = rk4_step(s64, i * dt, dt, rhs)
+        shi, slo = rk4_step_mixed(shi, i * dt, dt, rhs, slo)
+    torch.cuda.synchronize()
+    a, b, q0 = shi.q.cpu().numpy(), s64.q.cpu().numpy(), q64.cpu().numpy()
+
+    def rel(x, y):
+        # momentum components against the norm of the momentum field (the
+        # Taylor-Green z momentum starts at zero)
+        mom = np.linalg.norm(y[2:5].ravel())
+        return [float(np.linalg.norm((x[c] - y[c]).ravel()) /
+                      max(mom if 2 <= c < 5 else np.linalg.norm(y[c].ravel()), 1e-300))
+                for c in range(y.shape[0])]
+    return {"steps": nsteps, "dt": dt, "t_final": nsteps * dt,
+            "fields": ["mass", "energy", "momentum_x", "momentum_y", "momentum_z"],
+            "mixed_vs_fp64_rel_l2": rel(a, b), "fp64_change_rel_l2": rel(b, q0),
+            "wall_s": time.perf_counter() - t0}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -450,6 +502,10 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     status = runtime.read_status(dcoll, dev)
+    eor = None
+    if args.end_of_run > 0 and not mixture and world == 1 and not args.profile:
+        eor = _end_of_run(dcoll, gas, q64, args.end_of_run, w["n"])
+        status |= runtime.read_status(dcoll, dev)
     names = [f[0] for f in forms]
     tot = [res[n][0] for n in names]
     if world > 1:
@@ -553,6 +609,7 @@ def run_ours(args):
                                 "frac": ab64[top64] / (kt64[top64] / 1e3) / 1e9 / hbm,
                                 "algorithmic_bytes": ab64[top64], "traffic": traffic64},
         "device_status": status,
+        "end_of_run": eor,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
@@ -569,6 +626,10 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--end-of-run", type=int, default=0,
+                    help="after timing, run this many RK4 steps in the float64 and the "
+                         "mixed form and report their per-field difference (ideal-gas "
+                         "workloads)")
     ap.add_argument("--profile", action="store_true",
                     help="time the plain and mixed forms only (no network training, "
                          "end-to-end or CPU legs): the command profiled with ncu")
