@@ -418,9 +418,8 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
     }
     __syncthreads();
 
-    // phase 2: face values  fscale * (u* - u0)
-    for (int it = threadIdx.x; it < ne * NFN * NGU; it += blockDim.x) {
-      const int grp = it % NGU, fnode = it / NGU;
+    // phase 2: face values  fscale * (u* - u0), one face node per item
+    for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
       const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
       const int k = fn_s[fm];
       const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
@@ -433,7 +432,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
         const int en = cn >> 8, pr = cn & 255;
         const int kn = (pr < a.nperm) ? perm_s[pr * NFP + m] : NP;
         if (en >= E || kn >= NP) {
-          if (grp == 0) atomicOr(a.status, ST_BAD_INDEX);
+          atomicOr(a.status, ST_BAD_INDEX);
         } else {
           gi = (int64_t)en * NP + kn;
           mode = 0;
@@ -443,35 +442,30 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
         const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
         if (kind == BK_PRESCRIBED) {
           mode = 1;
-        } else if (kind < 0 && grp == 0) {
+        } else if (kind < 0) {
           atomicOr(a.status, ST_BAD_INDEX);
         }
       }
-      const int64_t bstride = (int64_t)a.nbf * NFP, bo = (int64_t)bf * NFP + m;
-      // exterior temperature (only the group holding field NC needs it)
-      R tp = R(0);
-      if (grp == NC / CG && mode != 2) {
-        if (MIX) {
-          tp = (mode == 0) ? a.t_op[gi] : a.bext[NC * bstride + bo];
-        } else {
-          R up[NC];
+      R* bcol = bs + e * KS + f * NFPK + m;
+      if (mode == 2) {
 #pragma unroll
-          for (int c = 0; c < NC; ++c) up[c] = (mode == 0) ? a.q[c * EN + gi] : a.bext[c * bstride + bo];
-          tp = node_temperature<R, DIM, NS>(up, R(0), g);
-        }
+        for (int c = 0; c < NU; ++c) bcol[c * EPB * KS] = fsc * bu[(c * EPB + e) * KU + k];
+        continue;
       }
+      const int64_t bstride = (int64_t)a.nbf * NFP, bo = (int64_t)bf * NFP + m;
+      R up[NU];
 #pragma unroll
-      for (int cc = 0; cc < CG; ++cc) {
-        const int c = grp * CG + cc;
-        if (c >= NU) break;
+      for (int c = 0; c < NC; ++c) up[c] = (mode == 0) ? a.q[c * EN + gi] : a.bext[c * bstride + bo];
+      if (MIX)
+        up[NC] = (mode == 0) ? a.t_op[gi] : a.bext[NC * bstride + bo];
+      else
+        up[NC] = node_temperature<R, DIM, NS>(up, R(0), g);
+#pragma unroll
+      for (int c = 0; c < NU; ++c) {
         const R um = bu[(c * EPB + e) * KU + k];           // u- - u0
         const R u0 = u0_s[c * EPB + e];
-        R v = um;
-        if (mode != 2) {
-          const R up = (c == NC) ? tp : (mode == 0 ? a.q[c * EN + gi] : a.bext[c * bstride + bo]);
-          v = (mode == 0) ? ((up - u0) + um) / R(2) : up - u0;
-        }
-        bs[(c * EPB + e) * KS + f * NFPK + m] = fsc * v;
+        const R v = (mode == 0) ? ((up[c] - u0) + um) / R(2) : up[c] - u0;
+        bcol[c * EPB * KS] = fsc * v;
       }
     }
     __syncthreads();
@@ -1198,9 +1192,9 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
       }
     }
 
-    // face terms
-    for (int it = threadIdx.x; it < ne * NFN * NG; it += blockDim.x) {
-      const int grp = it % NG, fnode = it / NG;
+    // face terms, one face node per item: the pairing and the wave speed
+    // once, then the field groups
+    for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
       const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
       const int k = fn_s[fm];
       const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
@@ -1229,26 +1223,29 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
           }
           lam = fmax(sqrt(vm2) + a.fbuf[gm * FW + LIM + 1], sqrt(vp2) + a.fbuf[gi * FW + LIM + 1]);
         }
-        R fmv[GV], fpv[GV], f0v[GV];
-        load_group<R, GV>(a.fbuf + gm * FW, grp * GV, LIM, fmv);
-        load_group<R, GV>(a.fbuf + gi * FW, grp * GV, LIM, fpv);
-        load_group<R, GV>(a.fbuf + g0 * FW, grp * GV, LIM, f0v);
+#pragma unroll 1
+        for (int grp = 0; grp < NG; ++grp) {
+          R fmv[GV], fpv[GV], f0v[GV];
+          load_group<R, GV>(a.fbuf + gm * FW, grp * GV, LIM, fmv);
+          load_group<R, GV>(a.fbuf + gi * FW, grp * GV, LIM, fpv);
+          load_group<R, GV>(a.fbuf + g0 * FW, grp * GV, LIM, f0v);
 #pragma unroll
-        for (int cc = 0; cc < CG; ++cc) {
-          const int c = grp * CG + cc;
-          if (c >= NC) break;
-          R sm_ = R(0), sp_ = R(0), s0 = R(0);
+          for (int cc = 0; cc < CG; ++cc) {
+            const int c = grp * CG + cc;
+            if (c >= NC) break;
+            R sm_ = R(0), sp_ = R(0), s0 = R(0);
 #pragma unroll
-          for (int j = 0; j < DIM; ++j) {
-            sm_ += fmv[cc * DIM + j] * n[j];
-            sp_ += fpv[cc * DIM + j] * n[j];
-            s0 += f0v[cc * DIM + j] * n[j];
+            for (int j = 0; j < DIM; ++j) {
+              sm_ += fmv[cc * DIM + j] * n[j];
+              sp_ += fpv[cc * DIM + j] * n[j];
+              s0 += f0v[cc * DIM + j] * n[j];
+            }
+            const R dq = a.q[c * EN + gm] - a.q[c * EN + gi];
+            const R out = (sm_ + sp_) / R(2) - lam * dq / R(2);
+            bcol[c * EPB * KB] = fsc * (out - s0);
           }
-          const R dq = a.q[c * EN + gm] - a.q[c * EN + gi];
-          const R out = (sm_ + sp_) / R(2) - lam * dq / R(2);
-          bcol[c * EPB * KB] = fsc * (out - s0);
         }
-      } else if (grp == 0) {
+      } else {
         surface_face_general<R, DIM, NP, NFP, NS, MIX, VISC>(
             a, g, EN, gm, g0, m, cn, n[0], n[1], DIM > 2 ? n[DIM - 1] : R(0), fsc, perm_s,
             bcol, EPB * KB);
