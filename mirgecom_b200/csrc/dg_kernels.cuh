@@ -1253,44 +1253,56 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
     }
     __syncthreads();
 
-    // rhs = [-W | LIFT] [G ; S] on the tensor cores (+ sources)
-    for (int w = warp; w < (NCOL / 8) * MT; w += nwarps) {
-      const int nt = w / MT, t = w % MT;
-      R d[NACC];
+    // rhs = [-W | LIFT] [G ; S] on the tensor cores (+ sources); one m-tile
+    // and NTG n-tiles per warp item, so each A fragment load serves NTG
+    // products
+    constexpr int NNT = NCOL / 8;
+    constexpr int NTG = (NNT % 3 == 0) ? 3 : ((NNT % 2 == 0) ? 2 : 1);
+    for (int w = warp; w < (NNT / NTG) * MT; w += nwarps) {
+      const int ng = w / MT, t = w % MT;
+      R d[NTG][NACC];
 #pragma unroll
-      for (int v = 0; v < NACC; ++v) d[v] = R(0);
-      const R* bcol = bm + (nt * 8 + gq) * KB + tq;
+      for (int u = 0; u < NTG; ++u)
+#pragma unroll
+        for (int v = 0; v < NACC; ++v) d[u][v] = R(0);
+      const R* bcol = bm + (ng * NTG * 8 + gq) * KB + tq;
       if constexpr (!C::TF32) {
 #pragma unroll 5
-        for (int ks = 0; ks < KRR / 4; ++ks)
-          dmma884(d, am[(t * 8 + gq) * KB + ks * 4 + tq], bcol[ks * 4]);
+        for (int ks = 0; ks < KRR / 4; ++ks) {
+          const double av = am[(t * 8 + gq) * KB + ks * 4 + tq];
+#pragma unroll
+          for (int u = 0; u < NTG; ++u) dmma884(d[u], av, bcol[u * 8 * KB + ks * 4]);
+        }
       } else {
 #pragma unroll 2
         for (int ks = 0; ks < KRR / 8; ++ks) {
-          const float b0 = bcol[ks * 8], b1 = bcol[ks * 8 + 4];
           uint32_t ah[4], alo[4];
           load_a_tf32(ah, am, KB, t * 16, ks * 8, gq, tq);
           load_a_tf32(alo, am + MP * KB, KB, t * 16, ks * 8, gq, tq);
-          mma_tf32x3(d, ah, alo, b0, b1);
+#pragma unroll
+          for (int u = 0; u < NTG; ++u)
+            mma_tf32x3(d[u], ah, alo, bcol[u * 8 * KB + ks * 8], bcol[u * 8 * KB + ks * 8 + 4]);
         }
       }
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int col = nt * 8 + 2 * tq + h;
-        const int c = col / EPB, e = col % EPB;
-        if (c >= NC || e >= ne) continue;
-        R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
+      for (int u = 0; u < NTG; ++u)
 #pragma unroll
-        for (int half = 0; half < NACC / 2; ++half) {
-          const int i = t * Tile<R>::MROW + gq + 8 * half;
-          if (i >= NP) continue;
-          R v = d[2 * half + h];
-          if (sources && c >= 2 + DIM)
-            v += a.srcbuf[(int64_t)(c - 2 - DIM) * EN + (int64_t)(e0 + e) * NP + i];
-          outp[i] = v;
-          bad |= !(v == v);
+        for (int h = 0; h < 2; ++h) {
+          const int col = (ng * NTG + u) * 8 + 2 * tq + h;
+          const int c = col / EPB, e = col % EPB;
+          if (c >= NC || e >= ne) continue;
+          R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
+#pragma unroll
+          for (int half = 0; half < NACC / 2; ++half) {
+            const int i = t * Tile<R>::MROW + gq + 8 * half;
+            if (i >= NP) continue;
+            R v = d[u][2 * half + h];
+            if (sources && c >= 2 + DIM)
+              v += a.srcbuf[(int64_t)(c - 2 - DIM) * EN + (int64_t)(e0 + e) * NP + i];
+            outp[i] = v;
+            bad |= !(v == v);
+          }
         }
-      }
     }
   }
   if (bad) atomicOr(a.status, ST_NAN);

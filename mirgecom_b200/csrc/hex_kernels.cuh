@@ -147,7 +147,6 @@ __global__ void __launch_bounds__(256, 2) k_hex_grad(DGArgs<R> a, GasParams g) {
   using H = Hex<ORDER>;
   constexpr int N1 = H::N1, NP = H::NP, NFP = H::NFP, NFN = H::NFN, NL = H::NL;
   constexpr int NC = C::NC, NU = C::NU, EPB = C::EPB_G, DIM = 3;
-  constexpr int CG = 4, NGU = (NU + CG - 1) / CG;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* u_s = reinterpret_cast<R*>(smem_raw);             // [EPB][NU][NP]
   R* s_s = u_s + EPB * NU * NP;                         // [EPB][NU][NF][NFP]
@@ -186,9 +185,8 @@ __global__ void __launch_bounds__(256, 2) k_hex_grad(DGArgs<R> a, GasParams g) {
     }
     __syncthreads();
 
-    // face values s' = u* - u0 per (face node, field group)
-    for (int it = threadIdx.x; it < ne * NFN * NGU; it += blockDim.x) {
-      const int grp = it % NGU, fnode = it / NGU;
+    // face values s' = u* - u0, one face node per item
+    for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
       const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
       const int k = hex_node<N1>(f >> 1, m, (f & 1) ? N1 - 1 : 0);
       const int cn = a.conn[(int64_t)(e0 + e) * 6 + f];
@@ -199,7 +197,7 @@ __global__ void __launch_bounds__(256, 2) k_hex_grad(DGArgs<R> a, GasParams g) {
         const int en = cn >> 8, pr = cn & 255;
         const int kn = (pr < a.nperm) ? perm_s[pr * NFP + m] : NP;
         if (en >= E || kn >= NP) {
-          if (grp == 0) atomicOr(a.status, ST_BAD_INDEX);
+          atomicOr(a.status, ST_BAD_INDEX);
         } else {
           gi = (int64_t)en * NP + kn;
           mode = 0;
@@ -209,34 +207,29 @@ __global__ void __launch_bounds__(256, 2) k_hex_grad(DGArgs<R> a, GasParams g) {
         const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
         if (kind == BK_PRESCRIBED)
           mode = 1;
-        else if (kind < 0 && grp == 0)
+        else if (kind < 0)
           atomicOr(a.status, ST_BAD_INDEX);
       }
-      const int64_t bstride = (int64_t)a.nbf * NFP, bo = (int64_t)bf * NFP + m;
-      R tp = R(0);
-      if (grp == NC / CG && mode != 2) {
-        if (MIX) {
-          tp = (mode == 0) ? a.t_op[gi] : a.bext[NC * bstride + bo];
-        } else {
-          R up[NC];
+      R* scol = s_s + e * NU * NFN + fm;
+      if (mode == 2) {
 #pragma unroll
-          for (int c = 0; c < NC; ++c)
-            up[c] = (mode == 0) ? a.q[c * EN + gi] : a.bext[c * bstride + bo];
-          tp = node_temperature<R, DIM, NS>(up, R(0), g);
-        }
+        for (int c = 0; c < NU; ++c)
+          scol[c * NFN] = u_s[(e * NU + c) * NP + k] - u_s[(e * NU + c) * NP];
+        continue;
       }
+      const int64_t bstride = (int64_t)a.nbf * NFP, bo = (int64_t)bf * NFP + m;
+      R up[NU];
 #pragma unroll
-      for (int cc = 0; cc < CG; ++cc) {
-        const int c = grp * CG + cc;
-        if (c >= NU) break;
+      for (int c = 0; c < NC; ++c) up[c] = (mode == 0) ? a.q[c * EN + gi] : a.bext[c * bstride + bo];
+      if (MIX)
+        up[NC] = (mode == 0) ? a.t_op[gi] : a.bext[NC * bstride + bo];
+      else
+        up[NC] = node_temperature<R, DIM, NS>(up, R(0), g);
+#pragma unroll
+      for (int c = 0; c < NU; ++c) {
         const R u0 = u_s[(e * NU + c) * NP];
         const R um = u_s[(e * NU + c) * NP + k] - u0;
-        R v = um;
-        if (mode != 2) {
-          const R up = (c == NC) ? tp : (mode == 0 ? a.q[c * EN + gi] : a.bext[c * bstride + bo]);
-          v = (mode == 0) ? ((up - u0) + um) / R(2) : up - u0;
-        }
-        s_s[(e * NU + c) * NFN + fm] = v;
+        scol[c * NFN] = (mode == 0) ? ((up[c] - u0) + um) / R(2) : up[c] - u0;
       }
     }
     __syncthreads();
@@ -357,9 +350,8 @@ __global__ void __launch_bounds__(256, 2) k_hex_surface(DGArgs<R> a, GasParams g
       }
     }
 
-    // faces: S = fsc (F* - F0) . n per (face node, field group)
-    for (int it = threadIdx.x; it < ne * NFN * NG; it += blockDim.x) {
-      const int grp = it % NG, fnode = it / NG;
+    // faces: S = fsc (F* - F0) . n, one face node per item
+    for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
       const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
       const int ax = f >> 1;
       const int k = hex_node<N1>(ax, m, (f & 1) ? N1 - 1 : 0);
@@ -396,26 +388,29 @@ __global__ void __launch_bounds__(256, 2) k_hex_surface(DGArgs<R> a, GasParams g
           }
           lam = fmax(sqrt(vm2) + a.fbuf[gm * FW + LIM + 1], sqrt(vp2) + a.fbuf[gi * FW + LIM + 1]);
         }
-        R fmv[GV], fpv[GV], f0v[GV];
-        load_group<R, GV>(a.fbuf + gm * FW, grp * GV, LIM, fmv);
-        load_group<R, GV>(a.fbuf + gi * FW, grp * GV, LIM, fpv);
-        load_group<R, GV>(a.fbuf + g0 * FW, grp * GV, LIM, f0v);
+#pragma unroll 1
+        for (int grp = 0; grp < NG; ++grp) {
+          R fmv[GV], fpv[GV], f0v[GV];
+          load_group<R, GV>(a.fbuf + gm * FW, grp * GV, LIM, fmv);
+          load_group<R, GV>(a.fbuf + gi * FW, grp * GV, LIM, fpv);
+          load_group<R, GV>(a.fbuf + g0 * FW, grp * GV, LIM, f0v);
 #pragma unroll
-        for (int cc = 0; cc < CG; ++cc) {
-          const int c = grp * CG + cc;
-          if (c >= NC) break;
-          R sm_ = R(0), sp_ = R(0), s0 = R(0);
+          for (int cc = 0; cc < CG; ++cc) {
+            const int c = grp * CG + cc;
+            if (c >= NC) break;
+            R sm_ = R(0), sp_ = R(0), s0 = R(0);
 #pragma unroll
-          for (int j = 0; j < DIM; ++j) {
-            sm_ += fmv[cc * DIM + j] * n[j];
-            sp_ += fpv[cc * DIM + j] * n[j];
-            s0 += f0v[cc * DIM + j] * n[j];
+            for (int j = 0; j < DIM; ++j) {
+              sm_ += fmv[cc * DIM + j] * n[j];
+              sp_ += fpv[cc * DIM + j] * n[j];
+              s0 += f0v[cc * DIM + j] * n[j];
+            }
+            const R dq = a.q[c * EN + gm] - a.q[c * EN + gi];
+            const R out = (sm_ + sp_) / R(2) - lam * dq / R(2);
+            bcol[c * NFN] = fsc * (out - s0);
           }
-          const R dq = a.q[c * EN + gm] - a.q[c * EN + gi];
-          const R out = (sm_ + sp_) / R(2) - lam * dq / R(2);
-          bcol[c * NFN] = fsc * (out - s0);
         }
-      } else if (grp == 0) {
+      } else {
         surface_face_general<R, DIM, NP, NFP, NS, MIX, VISC>(a, g, EN, gm, g0, m, cn, n[0], n[1],
                                                              n[2], fsc, perm_s, bcol, NFN);
       }
