@@ -203,6 +203,40 @@ __device__ __forceinline__ void mma_tf32x3(float (&d)[4], const uint32_t (&ahi)[
   mma_tf32(d, ahi, bh0, bh1);
 }
 
+// B operand split once into tf32 hi/lo words (shared by several A operands)
+struct SplitB {
+  uint32_t h0, h1, l0, l1;
+  __device__ __forceinline__ SplitB(float b0, float b1) {
+    h0 = to_tf32(b0);
+    h1 = to_tf32(b1);
+    l0 = to_tf32(b0 - __uint_as_float(h0));
+    l1 = to_tf32(b1 - __uint_as_float(h1));
+  }
+};
+
+// the same three-term product with B already split
+__device__ __forceinline__ void mma_tf32x3(float (&d)[4], const uint32_t (&ahi)[4],
+                                           const uint32_t (&alo)[4], const SplitB& b) {
+  mma_tf32(d, alo, b.h0, b.h1);
+  mma_tf32(d, ahi, b.l0, b.l1);
+  mma_tf32(d, ahi, b.h0, b.h1);
+}
+
+// A fragment of the tf32 m16n8k8 product (16 rows from m0, 8 columns from
+// k0, row stride `stride` floats, rows 16-byte aligned) in one ldmatrix.x4:
+// the four 8x8 b16 matrices are the 8x4-word blocks (rows 0-7 | 8-15) x
+// (k 0-3 | 4-7); lane l gives the row address of block l / 8, and receives
+// word (l % 4) of row (l / 4) of each block -- exactly a0..a3.
+__device__ __forceinline__ void load_a_tf32_ldsm(uint32_t (&a)[4], const float* am, int stride,
+                                                 int m0, int k0, int lane) {
+  const int row = m0 + (lane & 7) + ((lane >> 3) & 1) * 8;
+  const int kk = k0 + ((lane >> 4) << 2);
+  const uint32_t addr = (uint32_t)__cvta_generic_to_shared(am + row * stride + kk);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
+               : "r"(addr));
+}
+
 // hi/lo tf32 split of a float64 reference-matrix entry
 __device__ __forceinline__ void split_tf32(double v, float& hi, float& lo) {
   hi = __uint_as_float(to_tf32((float)v));
@@ -352,7 +386,6 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
   constexpr int KU = C::KU, KS = C::KS, KL = C::KL, NFPK = C::NFPK, NCOL = C::NCOL_G;
   constexpr int KUR = C::KUR;
   constexpr int AWN = DIM * MP * KU, ALN = NF * MP * KL;
-  constexpr int CG = 4, NGU = (NU + CG - 1) / CG;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* aw = reinterpret_cast<R*>(smem_raw);                  // [NAC][DIM][MP][KU]
   R* al = aw + NAC * AWN;                                  // [NAC][NF][MP][KL]
@@ -497,26 +530,28 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
           for (int ks = 0; ks < NFPK / 4; ++ks)
             dmma884(lf[f], al[(f * MP + t * 8 + gq) * KL + ks * 4 + tq], scol[f * NFPK + ks * 4]);
       } else {
+        // B split once per k-step and shared by the DIM operators; A
+        // fragments by ldmatrix
 #pragma unroll
         for (int ks = 0; ks < KUR / 8; ++ks) {
-          const float b0 = bcol[ks * 8], b1 = bcol[ks * 8 + 4];
+          const SplitB b(bcol[ks * 8], bcol[ks * 8 + 4]);
 #pragma unroll
           for (int r = 0; r < DIM; ++r) {
             uint32_t ah[4], alo[4];
-            load_a_tf32(ah, aw + r * MP * KU, KU, t * 16, ks * 8, gq, tq);
-            load_a_tf32(alo, aw + AWN + r * MP * KU, KU, t * 16, ks * 8, gq, tq);
-            mma_tf32x3(du[r], ah, alo, b0, b1);
+            load_a_tf32_ldsm(ah, aw + r * MP * KU, KU, t * 16, ks * 8, lane);
+            load_a_tf32_ldsm(alo, aw + AWN + r * MP * KU, KU, t * 16, ks * 8, lane);
+            mma_tf32x3(du[r], ah, alo, b);
           }
         }
 #pragma unroll
         for (int f = 0; f < NF; ++f)
 #pragma unroll
           for (int ks = 0; ks < NFPK / 8; ++ks) {
-            const float b0 = scol[f * NFPK + ks * 8], b1 = scol[f * NFPK + ks * 8 + 4];
+            const SplitB b(scol[f * NFPK + ks * 8], scol[f * NFPK + ks * 8 + 4]);
             uint32_t ah[4], alo[4];
-            load_a_tf32(ah, al + f * MP * KL, KL, t * 16, ks * 8, gq, tq);
-            load_a_tf32(alo, al + ALN + f * MP * KL, KL, t * 16, ks * 8, gq, tq);
-            mma_tf32x3(lf[f], ah, alo, b0, b1);
+            load_a_tf32_ldsm(ah, al + f * MP * KL, KL, t * 16, ks * 8, lane);
+            load_a_tf32_ldsm(alo, al + ALN + f * MP * KL, KL, t * 16, ks * 8, lane);
+            mma_tf32x3(lf[f], ah, alo, b);
           }
       }
 #pragma unroll
@@ -1277,8 +1312,8 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
 #pragma unroll 2
         for (int ks = 0; ks < KRR / 8; ++ks) {
           uint32_t ah[4], alo[4];
-          load_a_tf32(ah, am, KB, t * 16, ks * 8, gq, tq);
-          load_a_tf32(alo, am + MP * KB, KB, t * 16, ks * 8, gq, tq);
+          load_a_tf32_ldsm(ah, am, KB, t * 16, ks * 8, lane);
+          load_a_tf32_ldsm(alo, am + MP * KB, KB, t * 16, ks * 8, lane);
 #pragma unroll
           for (int u = 0; u < NTG; ++u)
             mma_tf32x3(d[u], ah, alo, bcol[u * 8 * KB + ks * 8], bcol[u * 8 * KB + ks * 8 + 4]);
