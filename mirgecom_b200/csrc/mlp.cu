@@ -20,6 +20,7 @@
 // output-layer gradients), the weight gradients as split-K products over
 // the samples (k_mlp_wgrad), and Adam (k_mlp_adam).
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -59,6 +60,19 @@ __device__ __forceinline__ float tanh_fast(float x) {
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(x * 2.8853900817779268f));
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e + 1.0f));
   return fmaf(-2.0f, r, 1.0f);
+}
+
+// Inference activations: two tanh per special-function operation
+// (tanh.approx.f16x2: f16 arguments and results, maximum relative error about
+// 2^-11).  The guess only seeds the Newton solve, whose accepted temperature
+// does not depend on where it started; training keeps tanh_fast.
+__device__ __forceinline__ void tanh2_infer(float x0, float x1, float& y0, float& y1) {
+  const __half2 h = __floats2half2_rn(x0, x1);
+  uint32_t in = *reinterpret_cast<const uint32_t*>(&h), out;
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(out) : "r"(in));
+  const __half2 r = *reinterpret_cast<const __half2*>(&out);
+  y0 = __low2float(r);
+  y1 = __high2float(r);
 }
 
 __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
@@ -193,8 +207,11 @@ __device__ __forceinline__ void forward_tile_y(const __nv_bfloat16* xs,
     mma_bf16(d, a0, a1, a2, a3, *reinterpret_cast<const uint32_t*>(wr + 2 * t),
              *reinterpret_cast<const uint32_t*>(wr + 2 * t + 8));
     const float bb0 = bias[nt * 8 + 2 * t], bb1 = bias[nt * 8 + 2 * t + 1];
-    hp[nt][0] = pack_bf16(tanh_fast(d[0] + bb0), tanh_fast(d[1] + bb1));
-    hp[nt][1] = pack_bf16(tanh_fast(d[2] + bb0), tanh_fast(d[3] + bb1));
+    float h0, h1, h2, h3;
+    tanh2_infer(d[0] + bb0, d[1] + bb1, h0, h1);
+    tanh2_infer(d[2] + bb0, d[3] + bb1, h2, h3);
+    hp[nt][0] = pack_bf16(h0, h1);
+    hp[nt][1] = pack_bf16(h2, h3);
   }
   float s0 = 0.f, s1 = 0.f;
 #pragma unroll
@@ -208,8 +225,11 @@ __device__ __forceinline__ void forward_tile_y(const __nv_bfloat16* xs,
                *reinterpret_cast<const uint32_t*>(wr + kk * 16 + 2 * t + 8));
     const float bb0 = bias[H + nt * 8 + 2 * t], bb1 = bias[H + nt * 8 + 2 * t + 1];
     const float w0 = bias[2 * H + nt * 8 + 2 * t], w1v = bias[2 * H + nt * 8 + 2 * t + 1];
-    s0 += w0 * tanh_fast(d[0] + bb0) + w1v * tanh_fast(d[1] + bb1);
-    s1 += w0 * tanh_fast(d[2] + bb0) + w1v * tanh_fast(d[3] + bb1);
+    float h0, h1, h2, h3;
+    tanh2_infer(d[0] + bb0, d[1] + bb1, h0, h1);
+    tanh2_infer(d[2] + bb0, d[3] + bb1, h2, h3);
+    s0 += w0 * h0 + w1v * h1;
+    s1 += w0 * h2 + w1v * h3;
   }
   s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
   s0 += __shfl_xor_sync(0xffffffffu, s0, 2);

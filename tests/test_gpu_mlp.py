@@ -58,10 +58,13 @@ def test_training_and_iteration_gain(cuda):
     p = net.numpy_params()
     x = net.features(e2, y2).cpu().numpy().astype(np.float64)
     ref = net.out_shift + net.out_scale * omlp.forward(p, x, emulate_bf16=True)["y"]
-    # identical up to bf16 rounding flips of the inputs: the device derives
-    # the features from the float32 state, the oracle from float64 (e, Y)
+    # inference evaluates tanh with tanh.approx.f16x2 (about 2^-11 relative
+    # error per activation, which also moves some bf16 roundings of the
+    # layer-1 activations by one step), and the device derives the features
+    # from the float32 state, the oracle from float64 (e, Y): a few kelvin at
+    # most, against the hundreds of kelvin a fragment-layout error would give
     d = np.abs(guess.cpu().numpy() - ref)
-    assert np.quantile(d, 0.99) < 0.05 and d.max() < 5.0, (np.quantile(d, 0.99), d.max())
+    assert np.quantile(d, 0.99) < 5.0 and d.max() < 25.0, (np.quantile(d, 0.99), d.max())
     # Newton iterations: reference default cold guess (300 K) vs learned guess
     gas_plain = GasModel(eos=PyrometheusMixture(UIUC_7SP))
     gas_learn = GasModel(eos=PyrometheusMixture(UIUC_7SP, learned_guess=net))
