@@ -381,9 +381,12 @@ def _newton_stats(dcoll, gas, q, tseed):
     it = torch.zeros(q[0].shape, dtype=torch.int32, device=q.device)
     make_fluid_state(ConservedVars(q, 3), gas, temperature_seed=tseed, newton_iterations=it)
     fb = it >= 1000
-    base = torch.where(fb, it - 1000, it).float()
+    base = torch.where(fb, it - 1000, it)
+    warm = base >= 100            # learned form: network skipped for a warm warp
+    base = torch.where(warm, base - 100, base).float()
     return {"mean": float(base.mean()), "max": int(base.max()),
-            "fallback_nodes": int(fb.sum())}
+            "fallback_nodes": int(fb.sum()),
+            "network_skipped_nodes": int(warm.sum()), "nodes": int(it.numel())}
 
 
 def _train_guess(dev, seed=0, steps=2000, samples=1 << 20):

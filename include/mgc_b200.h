@@ -259,8 +259,11 @@ int mgc_mlp_refresh(const mgc_mlp_t* w, void* stream);
 /* Mixed-form mixture temperature with the learned guess computed in the same
  * kernel (no counterpart in the reference, which has no learned guess): per
  * node the network's guess, then the solve of mgc_mixture_temperature_f32
- * with t_seed as the fallback.  Same arguments and status as that call plus
- * the network w; requires mgc_set_mechanism. */
+ * with t_seed as the fallback.  Nodes are taken 32 at a time: when the first
+ * Newton step from t_seed is at most 4 K for all 32 (a seed the network cannot
+ * improve on), the network is skipped and the solve continues from the seed;
+ * iters then carries + 100.  Same arguments and status as
+ * mgc_mixture_temperature_f32 plus the network w; requires mgc_set_mechanism. */
 int mgc_mixture_temperature_learned_f32(int dim, const mgc_gas_t* gas, int64_t nnodes,
                                         const float* q, const float* t_seed,
                                         const mgc_mlp_t* w, float* t_out, int32_t* iters,

@@ -65,6 +65,12 @@ __host__ __device__ constexpr int imin(int a, int b) { return a < b ? a : b; }
 __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
+// Flux record of the split divergence: NC*DIM total-flux values, then p, c,
+// gamma and the node's wave speed |v| + c, padded to 16 bytes.
+__host__ __device__ constexpr int flux_record_width(int dim, int nc) {
+  return round_up(nc * dim + 4, 4);
+}
+
 // Tensor-core tiling per arithmetic type.
 //   double: mma.m8n8k4.f64        -- m-tile 8,  k-step 4, 8-byte banks;
 //   float : mma.m16n8k8.tf32 x 3  -- m-tile 16, k-step 8, 4-byte banks.
@@ -133,9 +139,9 @@ struct Cfg {
   static constexpr int NCOL_R = round_up(NC * EPB_RHS, 8);
 
   // split right-hand side: per-node flux record = total flux F[c][j] then
-  // p, c, gamma (padded to 16 bytes); the surface kernel holds only the
-  // contraction operands in shared memory
-  static constexpr int FW = round_up(NC * DIM + 3, 4);
+  // p, c, gamma, |v| + c (padded to 16 bytes); the surface kernel holds only
+  // the contraction operands in shared memory
+  static constexpr int FW = flux_record_width(DIM, NC);
   static constexpr int S_BUDGET = (RB == 8 ? 100 : 74) * 1024;
   // resident blocks: float64 mixture state needs more registers per thread
   static constexpr int MINB_NODE = (RB == 8 && NS > 2) ? 3 : 4;
@@ -146,14 +152,14 @@ struct Cfg {
                                                                   : EPB_S_RAW / 4 * 4));
   static constexpr int NCOL_S = round_up(NC * EPB_SURF, 8);
   static size_t smem_surface(int nperm) {
-    return (size_t)(R_MAT + NCOL_S * KB + EPB_SURF * GEO) * RB + NFN * 4 + (size_t)nperm * NFP +
-           64;
+    return (size_t)(R_MAT + NCOL_S * KB + EPB_SURF * GEO) * RB + NFN * 4 + EPB_SURF * NF * 4 +
+           (size_t)nperm * NFP + 64;
   }
 
   static constexpr int MINB_GRAD = 2;
   static size_t smem_grad(int nperm) {
     return (size_t)(G_MAT + NCOL_G * (KU + KS) + EPB_GRAD * GEO + NU * EPB_GRAD) * RB +
-           NFN * 4 + (size_t)nperm * NFP + 64;
+           NFN * 4 + EPB_GRAD * NF * 4 + (size_t)nperm * NFP + 64;
   }
   static size_t smem_rhs(int nperm) {
     return (size_t)(R_MAT + NCOL_R * KB +
@@ -301,6 +307,16 @@ __device__ __forceinline__ void load_geometry(const R* __restrict__ rx_g, int e0
   }
 }
 
+// Face pairing of the tile's elements into shared memory (read back after
+// the next barrier), so that a face-node item starts its neighbour gathers
+// one global-memory round trip earlier.
+template <int NF>
+__device__ __forceinline__ void stage_conn(const int32_t* __restrict__ conn_g, int e0, int ne,
+                                           int32_t* conn_s) {
+  for (int idx = threadIdx.x; idx < ne * NF; idx += blockDim.x)
+    conn_s[idx] = conn_g[(int64_t)e0 * NF + idx];
+}
+
 // {{{ mixture temperature
 
 // plain form: T1 = Newton(seed), T2 = Newton(T1), fixed iteration count
@@ -396,7 +412,8 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
   R* fs_s = nrm_s + EPB * NF * DIM;                        // [EPB][NF]
   R* u0_s = fs_s + EPB * NF;                               // [NU][EPB]
   int* fn_s = reinterpret_cast<int*>(u0_s + NU * EPB);     // [NF*NFP]
-  uint8_t* perm_s = reinterpret_cast<uint8_t*>(fn_s + NFN);
+  int32_t* conn_s = fn_s + NFN;                            // [EPB][NF]
+  uint8_t* perm_s = reinterpret_cast<uint8_t*>(conn_s + EPB * NF);
 
   const int E = a.nelem;
   const int64_t EN = (int64_t)E * NP;
@@ -426,6 +443,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
     const int ne = imin(EPB, E - e0);
     // (its first barrier also orders the previous tile's contraction reads
     // of bu / bs before this tile's writes)
+    stage_conn<NF>(a.conn, e0, ne, conn_s);
     load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
 
     // phase 1: shifted conserved fields and temperature
@@ -455,7 +473,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
     for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
       const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
       const int k = fn_s[fm];
-      const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
+      const int cn = conn_s[e * NF + f];
       const R fsc = fs_s[e * NF + f];
       // 0: two-sided average with node gi; 1: prescribed exterior; 2: interior value
       int mode = 2;
@@ -887,11 +905,6 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
 // The split trades one record write + read per node for the 2-3x repeated
 // neighbour-state evaluations of the fused kernel.
 
-// Flux record width: NC*DIM total-flux values, then p, c, gamma, padded to 16 bytes.
-__host__ __device__ constexpr int flux_record_width(int dim, int nc) {
-  return round_up(nc * dim + 3, 4);
-}
-
 // resident 128-thread blocks of the node-flux kernel: the float64 mixture
 // state needs more registers per thread
 __host__ __device__ constexpr int node_flux_minb(int rb, int ns) { return (rb == 8 && ns > 2) ? 3 : 4; }
@@ -939,8 +952,14 @@ __global__ void __launch_bounds__(128, node_flux_minb((int)sizeof(R), NS))
     rec[NC * DIM] = st.p;
     rec[NC * DIM + 1] = st.c;
     rec[NC * DIM + 2] = st.gamma;
+    {
+      R v2 = R(0);
 #pragma unroll
-    for (int i = NC * DIM + 3; i < FW; ++i) rec[i] = R(0);
+      for (int j = 0; j < DIM; ++j) v2 += st.v[j] * st.v[j];
+      rec[NC * DIM + 3] = sqrt(v2) + st.c;
+    }
+#pragma unroll
+    for (int i = NC * DIM + 4; i < FW; ++i) rec[i] = R(0);
     bad |= !(st.p == st.p) || !(st.c == st.c);
     R* dst = a.fbuf + n * FW;
     if constexpr (sizeof(R) == 4) {
@@ -1140,8 +1159,11 @@ __device__ __noinline__ void surface_face_general(const DGArgs<R> a, const GasPa
 //           with the Rusanov or central flux the records already hold the
 //           total flux F = F_V - F_I on both sides, so
 //               F*_V - F*_I = (F^- + F^+) . n / 2 - lambda (q^- - q^+) / 2
-//           (lambda = max(|v| + c) for Rusanov, 0 for central): no face
-//           state is rebuilt.  Other faces take surface_face_general.
+//           (lambda = max(|v| + c) for Rusanov, the node wave speeds the
+//           records carry; 0 for central): no face state is rebuilt.  Other
+//           faces take surface_face_general.  The tile's face pairing is
+//           read from shared memory, so the neighbour gathers start one
+//           global round trip earlier.
 //   lift    rhs = [-W | LIFT] [G ; S] on the tensor cores, one (n-tile,
 //           m-tile) per warp work item, plus the species sources.
 // F0 is the record of the element's node 0: subtracting an element-constant
@@ -1166,7 +1188,8 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
   R* nrm_s = rx_s + EPB * DIM * DIM;
   R* fs_s = nrm_s + EPB * NF * DIM;
   int* fn_s = reinterpret_cast<int*>(fs_s + EPB * NF);
-  uint8_t* perm_s = reinterpret_cast<uint8_t*>(fn_s + NFN);
+  int32_t* conn_s = fn_s + NFN;
+  uint8_t* perm_s = reinterpret_cast<uint8_t*>(conn_s + EPB * NF);
 
   const int E = a.nelem;
   const int64_t EN = (int64_t)E * NP;
@@ -1201,6 +1224,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
     const int ne = imin(EPB, E - e0);
     // (its first barrier also orders the previous tile's contraction reads
     // of bm before this tile's writes)
+    stage_conn<NF>(a.conn, e0, ne, conn_s);
     load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
     __syncthreads();
 
@@ -1232,7 +1256,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
     for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
       const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
       const int k = fn_s[fm];
-      const int cn = a.conn[(int64_t)(e0 + e) * NF + f];
+      const int cn = conn_s[e * NF + f];
       const R fsc = fs_s[e * NF + f];
       R n[DIM];
 #pragma unroll
@@ -1246,18 +1270,9 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
         if (en < E && kn < NP) gi = (int64_t)en * NP + kn;
       }
       if (gi >= 0) {
-        R lam = R(0);
-        if (a.flux_kind == FLUX_RUSANOV) {
-          const R irm = R(1) / a.q[gm], irp = R(1) / a.q[gi];
-          R vm2 = R(0), vp2 = R(0);
-#pragma unroll
-          for (int j = 0; j < DIM; ++j) {
-            const R vm = a.q[(2 + j) * EN + gm] * irm, vp = a.q[(2 + j) * EN + gi] * irp;
-            vm2 += vm * vm;
-            vp2 += vp * vp;
-          }
-          lam = fmax(sqrt(vm2) + a.fbuf[gm * FW + LIM + 1], sqrt(vp2) + a.fbuf[gi * FW + LIM + 1]);
-        }
+        // Rusanov: lambda = max(|v| + c) of the two sides, from the records
+        const R lm = a.fbuf[gm * FW + LIM + 3], lp = a.fbuf[gi * FW + LIM + 3];
+        const R lam = (a.flux_kind == FLUX_RUSANOV) ? fmax(lm, lp) : R(0);
 #pragma unroll 1
         for (int grp = 0; grp < NG; ++grp) {
           R fmv[GV], fpv[GV], f0v[GV];

@@ -132,10 +132,12 @@ struct HexCfg {
   static constexpr int EPB_G = imax(1, imin(4, (BUDGET - NW * 3 * H::NP) / G_ELEM));
   static constexpr int EPB_S = imax(1, imin(4, (BUDGET - NW * H::NP) / S_ELEM));
   static size_t smem_grad(int nperm) {
-    return (size_t)(EPB_G * G_ELEM + NW * 3 * H::NP) * RB + (size_t)nperm * H::NFP + 64;
+    return (size_t)(EPB_G * G_ELEM + NW * 3 * H::NP) * RB + EPB_G * 6 * 4 +
+           (size_t)nperm * H::NFP + 64;
   }
   static size_t smem_surface(int nperm) {
-    return (size_t)(EPB_S * S_ELEM + NW * H::NP) * RB + (size_t)nperm * H::NFP + 64;
+    return (size_t)(EPB_S * S_ELEM + NW * H::NP) * RB + EPB_S * 6 * 4 +
+           (size_t)nperm * H::NFP + 64;
   }
 };
 
@@ -152,7 +154,8 @@ __global__ void __launch_bounds__(256, 2) k_hex_grad(DGArgs<R> a, GasParams g) {
   R* s_s = u_s + EPB * NU * NP;                         // [EPB][NU][NF][NFP]
   R* rx_s = s_s + EPB * NU * NFN;                       // [EPB][9]
   R* acc_all = rx_s + EPB * 9;                          // [NW][3][NP]
-  uint8_t* perm_s = reinterpret_cast<uint8_t*>(acc_all + C::NW * 3 * NP);
+  int32_t* conn_s = reinterpret_cast<int32_t*>(acc_all + C::NW * 3 * NP);  // [EPB][6]
+  uint8_t* perm_s = reinterpret_cast<uint8_t*>(conn_s + EPB * 6);
 
   const int E = a.nelem;
   const int64_t EN = (int64_t)E * NP;
@@ -171,6 +174,7 @@ __global__ void __launch_bounds__(256, 2) k_hex_grad(DGArgs<R> a, GasParams g) {
     __syncthreads();   // the previous tile's contraction reads are done
     for (int i = threadIdx.x; i < ne * 9; i += blockDim.x)
       rx_s[i] = a.rx[(int64_t)e0 * 9 + i];
+    stage_conn<6>(a.conn, e0, ne, conn_s);
     // conserved fields and temperature of the tile
     for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
       const int e = idx / NP, k = idx % NP;
@@ -189,7 +193,7 @@ __global__ void __launch_bounds__(256, 2) k_hex_grad(DGArgs<R> a, GasParams g) {
     for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
       const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
       const int k = hex_node<N1>(f >> 1, m, (f & 1) ? N1 - 1 : 0);
-      const int cn = a.conn[(int64_t)(e0 + e) * 6 + f];
+      const int cn = conn_s[e * 6 + f];
       int mode = 2;   // 0 two-sided average, 1 prescribed exterior, 2 interior value
       int64_t gi = 0;
       int bf = 0;
@@ -305,7 +309,8 @@ __global__ void __launch_bounds__(256, 2) k_hex_surface(DGArgs<R> a, GasParams g
   R* s_s = g_s + EPB * NC * 3 * NP;                     // [EPB][NC][NF][NFP]
   R* rx_s = s_s + EPB * NC * NFN;                       // [EPB][9]
   R* acc_all = rx_s + EPB * 9;                          // [NW][NP]
-  uint8_t* perm_s = reinterpret_cast<uint8_t*>(acc_all + C::NW * NP);
+  int32_t* conn_s = reinterpret_cast<int32_t*>(acc_all + C::NW * NP);  // [EPB][6]
+  uint8_t* perm_s = reinterpret_cast<uint8_t*>(conn_s + EPB * 6);
 
   const int E = a.nelem;
   const int64_t EN = (int64_t)E * NP;
@@ -326,6 +331,7 @@ __global__ void __launch_bounds__(256, 2) k_hex_surface(DGArgs<R> a, GasParams g
     __syncthreads();
     for (int i = threadIdx.x; i < ne * 9; i += blockDim.x)
       rx_s[i] = a.rx[(int64_t)e0 * 9 + i];
+    stage_conn<6>(a.conn, e0, ne, conn_s);
     __syncthreads();
 
     // volume: G_a = sum_j rx[a][j] (F_j - F0_j)
@@ -355,7 +361,7 @@ __global__ void __launch_bounds__(256, 2) k_hex_surface(DGArgs<R> a, GasParams g
       const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
       const int ax = f >> 1;
       const int k = hex_node<N1>(ax, m, (f & 1) ? N1 - 1 : 0);
-      const int cn = a.conn[(int64_t)(e0 + e) * 6 + f];
+      const int cn = conn_s[e * 6 + f];
       // n dS = J rx^T N dS_ref: the normal is +-rx[ax][:] normalised
       R n[3], mag2 = R(0);
 #pragma unroll
@@ -376,18 +382,9 @@ __global__ void __launch_bounds__(256, 2) k_hex_surface(DGArgs<R> a, GasParams g
         if (en < E && kn < NP) gi = (int64_t)en * NP + kn;
       }
       if (gi >= 0) {
-        R lam = R(0);
-        if (a.flux_kind == FLUX_RUSANOV) {
-          const R irm = R(1) / a.q[gm], irp = R(1) / a.q[gi];
-          R vm2 = R(0), vp2 = R(0);
-#pragma unroll
-          for (int j = 0; j < DIM; ++j) {
-            const R vm = a.q[(2 + j) * EN + gm] * irm, vp = a.q[(2 + j) * EN + gi] * irp;
-            vm2 += vm * vm;
-            vp2 += vp * vp;
-          }
-          lam = fmax(sqrt(vm2) + a.fbuf[gm * FW + LIM + 1], sqrt(vp2) + a.fbuf[gi * FW + LIM + 1]);
-        }
+        // Rusanov: lambda = max(|v| + c) of the two sides, from the records
+        const R lm = a.fbuf[gm * FW + LIM + 3], lp = a.fbuf[gi * FW + LIM + 3];
+        const R lam = (a.flux_kind == FLUX_RUSANOV) ? fmax(lm, lp) : R(0);
 #pragma unroll 1
         for (int grp = 0; grp < NG; ++grp) {
           R fmv[GV], fpv[GV], f0v[GV];

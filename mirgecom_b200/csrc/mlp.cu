@@ -554,13 +554,22 @@ int grid_for(int64_t tiles) {
 
 // {{{ mixture temperature with the learned guess (fused)
 
-// One warp per 32 nodes: the network runs on the warp's two 16-sample tiles
-// (features from the node's float64 energy and mass fractions), the guesses
-// go through shared memory, and each lane then solves its node's
-// temperature with mixed_newton from the guess, falling back to the seed
-// when the float64 residual check fails (iteration count + 1000 marks it).
+// A seed whose first Newton step is at most this large already needs no more
+// float32 steps than a network guess would (the step after it is below
+// k dT^2 = 0.05 K, and the trained network's validation error is larger than
+// this), so a warp whose seeds all pass skips the network.
+constexpr float kWarmSeedK = 4.0f;
+
+// One warp per 32 nodes.  First every lane takes one float32 Newton step
+// from its seed; when all the warp's steps are within kWarmSeedK the solve
+// simply continues from there (iteration count + 100 marks these nodes).
+// Otherwise the network runs on the warp's two 16-sample tiles (features
+// from the node's float64 energy and mass fractions), the guesses go through
+// shared memory, and each lane solves its node's temperature with
+// mixed_newton from the guess, falling back to the seed when the float64
+// residual check fails (iteration count + 1000 marks it).
 template <int DIM, int NS>
-__global__ void __launch_bounds__(WARPS * 32) k_mixture_state_learned(
+__global__ void __launch_bounds__(WARPS * 32, 6) k_mixture_state_learned(
     int64_t n, const float* __restrict__ q, const float* __restrict__ tseed, Net net,
     float* __restrict__ tout, int32_t* __restrict__ iters, int maxit, double rtol,
     int32_t* __restrict__ status) {
@@ -582,7 +591,39 @@ __global__ void __launch_bounds__(WARPS * 32) k_mixture_state_learned(
        ch += (int64_t)gridDim.x * WARPS) {
     const int64_t s = ch * 32 + lane;
     const bool valid = s < n;
-    // the Newton inputs are derived twice (features here, the solve after the
+    {
+      // one float32 step from the seed; a warm warp finishes from there
+      float qq[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) qq[c] = valid ? q[(int64_t)c * n + s] : (c == 0 ? 1.f : 0.f);
+      float y[NS], e32;
+      double yd[NS], e64;
+      mixed_newton_inputs<DIM, NS>(qq, y, yd, e32, e64);
+      const float ts = valid ? tseed[s] : 1000.f;
+      float em, cv;
+      mixture_e_cv<float, NS>(y, ts, em, cv);
+      const float dt0 = (e32 - em) / cv;
+      const bool warm = !valid || (ts > 0.f && fabsf(dt0) <= kWarmSeedK);
+      if (__all_sync(0xffffffffu, warm)) {
+        if (valid) {
+          const float k = mech<float>().newton_k, rt = (float)rtol;
+          float t = ts + dt0;
+          int used = 1;
+          const bool stop = k * dt0 * dt0 <= 0.25f * sqrtf(rt * fabsf(t) / k);
+          bool ok = mixed_newton<NS>(y, yd, e32, e64, t, stop ? 0 : maxit - 1, rtol, used);
+          if (!ok) {
+            used += 1000;
+            t = ts;
+            ok = mixed_newton<NS>(y, yd, e32, e64, t, maxit, rtol, used);
+          }
+          if (!ok) miss = true;
+          tout[s] = t;
+          if (iters) iters[s] = used + 100;
+        }
+        continue;
+      }
+    }
+    // the Newton inputs are derived again (features here, the solve after the
     // network: the second read of q hits L1) so that none stays live across
     // the network
     {

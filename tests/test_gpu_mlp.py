@@ -84,3 +84,16 @@ def test_training_and_iteration_gain(cuda):
     both = ok_p & ok_l
     assert float(((tp - tl).abs() / tl)[both].max()) < 2e-6
     assert float(((tl.double() - t2).abs() / t2).max()) < 2e-6
+    # seeds within one small Newton step (time marching): every warp skips
+    # the network (+100 marker) and the temperatures are those of the plain
+    # solve from the same seeds
+    warm = t2 + 1.0
+    it_w = torch.zeros_like(it_plain)
+    it_wp = torch.zeros_like(it_plain)
+    tw = make_fluid_state(cv, gas_learn, temperature_seed=warm,
+                          newton_iterations=it_w).temperature
+    twp = make_fluid_state(cv, gas_plain, temperature_seed=warm,
+                           newton_iterations=it_wp).temperature
+    assert bool(((it_w >= 100) & (it_w < 1000)).all())
+    assert float((it_w - 100 != it_wp).float().mean()) < 1e-3
+    assert float(((tw - twp).abs() / twp).max()) < 2e-6
