@@ -217,11 +217,13 @@ inline int mixture_state_mixed_dim(int ns, int64_t nnodes, const float* q, const
                                    cudaStream_t s) {
   if (ns != 7) return MGC_E_UNSUPPORTED;
   const int nt = 256;
-  int64_t nb = (nnodes + nt - 1) / nt;
-  if (nb > 148 * 16) nb = 148 * 16;
-  if (nb < 1) nb = 1;
-  k_mixture_state_mixed<DIM, 7><<<(unsigned)nb, nt, 0, s>>>(nnodes, q, tseed, tguess, tout, iters,
-                                                           maxit, rtol, status, g);
+  // grid-stride loop: one wave of resident blocks, so that no second,
+  // partly filled wave runs at a fraction of the machine
+  auto kern = k_mixture_state_mixed<DIM, 7>;
+  int nb = 0;
+  const int rc = persistent_grid(kern, nt, 0, (nnodes + nt - 1) / nt, &nb);
+  if (rc) return rc;
+  kern<<<(unsigned)nb, nt, 0, s>>>(nnodes, q, tseed, tguess, tout, iters, maxit, rtol, status, g);
   return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
 }
 
@@ -230,10 +232,11 @@ inline int mixture_state_dim(int ns, int64_t nnodes, const R* q, const R* tseed,
                              const GasParams& g, cudaStream_t s) {
   if (ns != 7) return MGC_E_UNSUPPORTED;
   const int nt = 256;
-  int64_t nb = (nnodes + nt - 1) / nt;
-  if (nb > 148 * 16) nb = 148 * 16;
-  if (nb < 1) nb = 1;
-  k_mixture_state<R, DIM, 7><<<(unsigned)nb, nt, 0, s>>>(nnodes, q, tseed, t1, t2, g);
+  auto kern = k_mixture_state<R, DIM, 7>;   // grid-stride: one wave of resident blocks
+  int nb = 0;
+  const int rc = persistent_grid(kern, nt, 0, (nnodes + nt - 1) / nt, &nb);
+  if (rc) return rc;
+  kern<<<(unsigned)nb, nt, 0, s>>>(nnodes, q, tseed, t1, t2, g);
   return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
 }
 

@@ -122,7 +122,10 @@ struct Cfg {
   static constexpr int G_MAT = NAC * (DIM * MP * KU + NF * MP * KL);
   static constexpr int G_PER_ELEM = NU * (KU + KS + 1) + GEO;
   static constexpr int EPB_G_RAW = (SMEM_BUDGET / RB - G_MAT - 1024 / RB) / G_PER_ELEM;
-  static constexpr int EPB_GRAD = imax(8, imin(32, EPB_G_RAW / 8 * 8));
+  // elements per tile, a multiple of 4: the float32 7-species p3 tile of 12
+  // gives the 256 threads 240 nodes, 480 face nodes and 40 (n-tile, m-tile)
+  // items for the 8 warps, with little idle time at the tile's barriers
+  static constexpr int EPB_GRAD = imax(8, imin(32, EPB_G_RAW / 4 * 4));
   static constexpr int NCOL_G = round_up(NU * EPB_GRAD, 8);
 
   // rhs kernel operands: B [col][KB] = [G_0 .. G_{DIM-1} | S] per column,
@@ -142,14 +145,13 @@ struct Cfg {
   // p, c, gamma, |v| + c (padded to 16 bytes); the surface kernel holds only
   // the contraction operands in shared memory
   static constexpr int FW = flux_record_width(DIM, NC);
-  static constexpr int S_BUDGET = (RB == 8 ? 100 : 74) * 1024;
+  static constexpr int S_BUDGET = (RB == 8 ? 100 : 92) * 1024;
   // resident blocks: float64 mixture state needs more registers per thread
   static constexpr int MINB_NODE = (RB == 8 && NS > 2) ? 3 : 4;
   static constexpr int MINB_SURF = 2;
   static constexpr int S_PER_ELEM = NC * KB + GEO;
   static constexpr int EPB_S_RAW = (S_BUDGET / RB - R_MAT - 1024 / RB) / S_PER_ELEM;
-  static constexpr int EPB_SURF = imax(4, imin(32, EPB_S_RAW >= 8 ? EPB_S_RAW / 8 * 8
-                                                                  : EPB_S_RAW / 4 * 4));
+  static constexpr int EPB_SURF = imax(4, imin(32, EPB_S_RAW / 4 * 4));
   static constexpr int NCOL_S = round_up(NC * EPB_SURF, 8);
   static size_t smem_surface(int nperm) {
     return (size_t)(R_MAT + NCOL_S * KB + EPB_SURF * GEO) * RB + NFN * 4 + EPB_SURF * NF * 4 +
@@ -441,8 +443,9 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = tile * EPB;
     const int ne = imin(EPB, E - e0);
-    // (its first barrier also orders the previous tile's contraction reads
-    // of bu / bs before this tile's writes)
+    // the previous tile's phase 3 reads rx_s and nrm_s, which load_geometry
+    // overwrites before its own first barrier
+    __syncthreads();
     stage_conn<NF>(a.conn, e0, ne, conn_s);
     load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
 
@@ -1222,8 +1225,9 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = tile * EPB;
     const int ne = imin(EPB, E - e0);
-    // (its first barrier also orders the previous tile's contraction reads
-    // of bm before this tile's writes)
+    // (no barrier needed before these writes: the previous tile's last
+    // phase reads only am / bm, and the first barrier of load_geometry
+    // orders those reads before this tile's writes of bm)
     stage_conn<NF>(a.conn, e0, ne, conn_s);
     load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
     __syncthreads();

@@ -779,16 +779,18 @@ int mgc_mixture_temperature_learned_f32(int dim, const mgc_gas_t* gas, int64_t n
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MGC_E_CUDA;
   if (!g_mech_ready_mlp[dev]) return MGC_E_NOT_READY;
   const Net net = make_net(mlp);
-  const int nb = grid_for((nnodes + 31) / 32);
   cudaStream_t s = (cudaStream_t)stream;
-  if (dim == 3)
-    k_mixture_state_learned<3, 7><<<nb, WARPS * 32, 0, s>>>(nnodes, q, t_seed, net, t_out,
-                                                             iterations, maxit, (double)rtol,
-                                                             status);
-  else
-    k_mixture_state_learned<2, 7><<<nb, WARPS * 32, 0, s>>>(nnodes, q, t_seed, net, t_out,
-                                                             iterations, maxit, (double)rtol,
-                                                             status);
+  auto kern = dim == 3 ? k_mixture_state_learned<3, 7> : k_mixture_state_learned<2, 7>;
+  // grid-stride over 32-node chunks: one wave of resident blocks
+  int sms = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, 0) != cudaSuccess)
+    return MGC_E_CUDA;
+  const int64_t want = ((nnodes + 31) / 32 + WARPS - 1) / WARPS;
+  int64_t nb = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
+  if (nb > want) nb = want;
+  kern<<<(unsigned)(nb > 0 ? nb : 1), WARPS * 32, 0, s>>>(nnodes, q, t_seed, net, t_out,
+                                                          iterations, maxit, (double)rtol, status);
   return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
 }
 
