@@ -591,48 +591,25 @@ __global__ void __launch_bounds__(WARPS * 32, 6) k_mixture_state_learned(
        ch += (int64_t)gridDim.x * WARPS) {
     const int64_t s = ch * 32 + lane;
     const bool valid = s < n;
-    {
-      // one float32 step from the seed; a warm warp finishes from there
-      float qq[NC];
+    float qq[NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) qq[c] = valid ? q[(int64_t)c * n + s] : (c == 0 ? 1.f : 0.f);
-      float y[NS], e32;
-      double yd[NS], e64;
-      mixed_newton_inputs<DIM, NS>(qq, y, yd, e32, e64);
-      const float ts = valid ? tseed[s] : 1000.f;
-      float em, cv;
-      mixture_e_cv<float, NS>(y, ts, em, cv);
-      const float dt0 = (e32 - em) / cv;
-      const bool warm = !valid || (ts > 0.f && fabsf(dt0) <= kWarmSeedK);
-      if (__all_sync(0xffffffffu, warm)) {
-        if (valid) {
-          const float k = mech<float>().newton_k, rt = (float)rtol;
-          float t = ts + dt0;
-          int used = 1;
-          const bool stop = k * dt0 * dt0 <= 0.25f * sqrtf(rt * fabsf(t) / k);
-          bool ok = mixed_newton<NS>(y, yd, e32, e64, t, stop ? 0 : maxit - 1, rtol, used);
-          if (!ok) {
-            used += 1000;
-            t = ts;
-            ok = mixed_newton<NS>(y, yd, e32, e64, t, maxit, rtol, used);
-          }
-          if (!ok) miss = true;
-          tout[s] = t;
-          if (iters) iters[s] = used + 100;
-        }
-        continue;
-      }
-    }
-    // the Newton inputs are derived again (features here, the solve after the
-    // network: the second read of q hits L1) so that none stays live across
-    // the network
-    {
-      float qq[NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) qq[c] = valid ? q[(int64_t)c * n + s] : (c == 0 ? 1.f : 0.f);
-      float y[NS], e32;
-      double yd[NS], e64;
-      mixed_newton_inputs<DIM, NS>(qq, y, yd, e32, e64);
+    for (int c = 0; c < NC; ++c) qq[c] = valid ? q[(int64_t)c * n + s] : (c == 0 ? 1.f : 0.f);
+    float y[NS], e32;
+    double yd[NS], e64;
+    mixed_newton_inputs<DIM, NS>(qq, y, yd, e32, e64);
+    // one float32 step from the seed; a warm warp continues from there
+    const float ts = valid ? tseed[s] : 1000.f;
+    float t, em, cv;
+    mixture_e_cv<float, NS>(y, ts, em, cv);
+    const float dt0 = (e32 - em) / cv;
+    int used, mx;
+    if (__all_sync(0xffffffffu, !valid || (ts > 0.f && fabsf(dt0) <= kWarmSeedK))) {
+      const float k = mech<float>().newton_k, rt = (float)rtol;
+      t = ts + dt0;
+      used = 101;        // one step, + 100: the network was skipped
+      mx = (k * dt0 * dt0 <= 0.25f * sqrtf(rt * fabsf(t) / k)) ? 0 : maxit - 1;
+    } else {
+      // network guess for the warp's 32 nodes (features from the inputs)
       float f[8];
       f[0] = e32;
 #pragma unroll
@@ -643,39 +620,39 @@ __global__ void __launch_bounds__(WARPS * 32, 6) k_mixture_state_learned(
         const float v1 = j + 1 < 8 ? (f[j + 1] - net.in_shift[j + 1]) * net.in_scale[j + 1] : 0.f;
         *reinterpret_cast<uint32_t*>(xs + lane * (KIN + 8) + j) = pack_bf16(v0, v1);
       }
-    }
-    __syncwarp();
+      __syncwarp();
 #pragma unroll 1
-    for (int half = 0; half < 2; ++half) {
-      float y0, y1;
-      forward_tile_y(xs + half * 16 * (KIN + 8), w1s, w2s, bias, y0, y1);
-      if ((lane & 3) == 0) {
-        const int g = lane >> 2;
-        tg[half * 16 + g] = net.out_shift + net.out_scale * y0;
-        tg[half * 16 + g + 8] = net.out_shift + net.out_scale * y1;
+      for (int half = 0; half < 2; ++half) {
+        float y0, y1;
+        forward_tile_y(xs + half * 16 * (KIN + 8), w1s, w2s, bias, y0, y1);
+        if ((lane & 3) == 0) {
+          const int g = lane >> 2;
+          tg[half * 16 + g] = net.out_shift + net.out_scale * y0;
+          tg[half * 16 + g + 8] = net.out_shift + net.out_scale * y1;
+        }
       }
-    }
-    __syncwarp();
-    if (valid) {
-      float qq[NC];
+      __syncwarp();
+      t = tg[lane];
+      used = 0;
+      mx = maxit;
+      __syncwarp();
+      // the Newton inputs are derived again (the second read of q hits L1),
+      // so that none of them stays live across the network
 #pragma unroll
-      for (int c = 0; c < NC; ++c) qq[c] = q[(int64_t)c * n + s];
-      float y[NS], e32;
-      double yd[NS], e64;
+      for (int c = 0; c < NC; ++c) qq[c] = valid ? q[(int64_t)c * n + s] : (c == 0 ? 1.f : 0.f);
       mixed_newton_inputs<DIM, NS>(qq, y, yd, e32, e64);
-      int used = 0;
-      float t = tg[lane];
-      bool ok = mixed_newton<NS>(y, yd, e32, e64, t, maxit, rtol, used);
+    }
+    if (valid) {
+      bool ok = mixed_newton<NS>(y, yd, e32, e64, t, mx, rtol, used);
       if (!ok) {
         used += 1000;
-        t = tseed[s];
+        t = ts;
         ok = mixed_newton<NS>(y, yd, e32, e64, t, maxit, rtol, used);
       }
       if (!ok) miss = true;
       tout[s] = t;
       if (iters) iters[s] = used;
     }
-    __syncwarp();
   }
   if (miss) atomicOr(status, ST_NEWTON_MISS);
 }
