@@ -419,6 +419,10 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
 
   const int E = a.nelem;
   const int64_t EN = (int64_t)E * NP;
+  // whole rows of NP floats can be moved in 16-byte pieces
+  const bool rows16 =
+      ((reinterpret_cast<uintptr_t>(a.q) | reinterpret_cast<uintptr_t>(a.t_op)) & 15) == 0 &&
+      (KU * sizeof(R)) % 16 == 0;
 
   // reference operators (zero padded; hi/lo tf32 split on the mixed path)
   for (int i = threadIdx.x; i < AWN; i += blockDim.x) {
@@ -449,25 +453,49 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
     stage_conn<NF>(a.conn, e0, ne, conn_s);
     load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
 
-    // phase 1: shifted conserved fields and temperature
-    for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
-      const int e = idx / NP, k = idx % NP;
-      const int64_t gn = (int64_t)e0 * NP + idx, g0 = (int64_t)(e0 + e) * NP;
-      R qq[NC], q0[NC];
+    // phase 1: shifted conserved fields and temperature.  With the operator
+    // temperature given (mixtures) one (element, field) row per item: the
+    // row's NP values in 16-byte loads, shifted by its first; otherwise one
+    // node per item (the ideal-gas temperature needs all fields of a node)
+    bool rows_done = false;
+    if constexpr (MIX && NP % 4 == 0 && sizeof(R) == 4) {
+      if (rows16) {
+        for (int it = threadIdx.x; it < ne * NU; it += blockDim.x) {
+          const int e = it % ne, c = it / ne;
+          const float* src = (c < NC ? a.q + c * EN : a.t_op) + (int64_t)(e0 + e) * NP;
+          float4 v[NP / 4];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        qq[c] = a.q[c * EN + gn];
-        q0[c] = a.q[c * EN + g0];
+          for (int i = 0; i < NP / 4; ++i) v[i] = reinterpret_cast<const float4*>(src)[i];
+          const float u0 = v[0].x;
+          float4* dst = reinterpret_cast<float4*>(bu + (c * EPB + e) * KU);
+#pragma unroll
+          for (int i = 0; i < NP / 4; ++i)
+            dst[i] = make_float4(v[i].x - u0, v[i].y - u0, v[i].z - u0, v[i].w - u0);
+          u0_s[c * EPB + e] = u0;
+        }
+        rows_done = true;
       }
-      const R t = MIX ? a.t_op[gn] : node_temperature<R, DIM, NS>(qq, R(0), g);
-      const R t0 = MIX ? a.t_op[g0] : node_temperature<R, DIM, NS>(q0, R(0), g);
+    }
+    if (!rows_done) {
+      for (int idx = threadIdx.x; idx < ne * NP; idx += blockDim.x) {
+        const int e = idx / NP, k = idx % NP;
+        const int64_t gn = (int64_t)e0 * NP + idx, g0 = (int64_t)(e0 + e) * NP;
+        R qq[NC], q0[NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) bu[(c * EPB + e) * KU + k] = qq[c] - q0[c];
-      bu[(NC * EPB + e) * KU + k] = t - t0;
-      if (k == 0) {
+        for (int c = 0; c < NC; ++c) {
+          qq[c] = a.q[c * EN + gn];
+          q0[c] = a.q[c * EN + g0];
+        }
+        const R t = MIX ? a.t_op[gn] : node_temperature<R, DIM, NS>(qq, R(0), g);
+        const R t0 = MIX ? a.t_op[g0] : node_temperature<R, DIM, NS>(q0, R(0), g);
 #pragma unroll
-        for (int c = 0; c < NC; ++c) u0_s[c * EPB + e] = q0[c];
-        u0_s[NC * EPB + e] = t0;
+        for (int c = 0; c < NC; ++c) bu[(c * EPB + e) * KU + k] = qq[c] - q0[c];
+        bu[(NC * EPB + e) * KU + k] = t - t0;
+        if (k == 0) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) u0_s[c * EPB + e] = q0[c];
+          u0_s[NC * EPB + e] = t0;
+        }
       }
     }
     __syncthreads();
