@@ -211,6 +211,19 @@ def _dist_env():
     return rank, world, local
 
 
+def _max_over_ranks(xs, device):
+    """Element-wise maximum of the float list *xs* over all ranks (the
+    device times of a multi-process run); *xs* itself when not distributed.
+    Every rank must call it at the same point."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(x) for x in xs]
+    t = torch.tensor([float(x) for x in xs], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def _oracle_setup(name):
     """Oracle discretization and gas of a bounded sample of the workload
     (numpy only; no torch, so spawned CPU workers stay light)."""
@@ -510,6 +523,15 @@ def _end_of_run_mixture(dcoll, gas, gas_head, q64, t64, nsteps, dt=5e-9):
 
 
 def run_ours(args):
+    import torch.distributed as dist
+    try:
+        _run_ours(args)
+    finally:
+        if dist.is_available() and dist.is_initialized():
+            dist.destroy_process_group()
+
+
+def _run_ours(args):
     import torch
     import torch.distributed as dist
 
@@ -569,11 +591,7 @@ def run_ours(args):
             eor = _end_of_run(dcoll, gas, q64, args.end_of_run, w["n"])
         status |= runtime.read_status(dcoll, dev)
     names = [f[0] for f in forms]
-    tot = [res[n][0] for n in names]
-    if world > 1:
-        tt = torch.tensor(tot, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        tot = [float(v) for v in tt.tolist()]
+    tot = _max_over_ranks([res[n][0] for n in names], dev)
     values = {n: world * dof * args.steps / (ms / 1e3) for n, ms in zip(names, tot)}
     head = "mixed_learned" if gas_learn is not None else "mixed_plain_guess"
     hq, ht, hgas = q32, t32, (gas_learn if gas_learn is not None else gas)
@@ -636,6 +654,7 @@ def run_ours(args):
         ev[1].record(stream)
         torch.cuda.synchronize()
         e2e_ms += ev[0].elapsed_time(ev[1])
+    e2e_ms = _max_over_ranks([e2e_ms], dev)[0]
     e2e_value = world * dof * args.steps / (e2e_ms / 1e3)
 
     # roofline of the dominant kernel of the headline form
@@ -702,8 +721,6 @@ def run_ours(args):
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
 
 
 def main(argv=None):
