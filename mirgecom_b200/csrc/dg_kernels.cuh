@@ -928,8 +928,8 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
 // {{{ split right-hand side: pointwise flux kernel + surface/lift kernel
 //
 // k_node_flux evaluates every node's state and total flux F = F_V - F_I once
-// (plus p, c, gamma and the Arrhenius sources) and writes a flux record per
-// node.  k_surface then builds, per element tile, the metric-combined volume
+// (plus p, c, gamma, the wave speed |v| + c and the Arrhenius sources) and
+// writes a flux record per node.  k_surface then builds, per element tile, the metric-combined volume
 // terms from the records, the numerical face fluxes from the records of both
 // sides of each face node (the neighbour's flux is gathered, not
 // recomputed), and contracts on the tensor cores exactly as k_rhs does.
