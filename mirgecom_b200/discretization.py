@@ -211,6 +211,29 @@ class Discretization:
         x = self.boundary_nodes_numpy()[:, mask]
         return torch.from_numpy(np.ascontiguousarray(x)).to(device or self.device)
 
+    def characteristic_lengthscales(self, device=None, dtype=None):
+        """Per-node length scale h = min(dr) r_D for time-step estimates
+        (grudge's ``dt_utils.characteristic_lengthscales``, after Hesthaven &
+        Warburton 2008, sec. 6.4): min(dr) is the smallest distance between
+        two nodes of the reference element (its [-1, 1] coordinates), r_D the
+        element's inradius d V / sum_f F_f (for an affine element the
+        Jacobian cancels: d V_ref / sum_f |rx^T N_f| F_ref,f).  Shape (E, Np)."""
+        import torch
+        key = ("char_len", str(device), str(dtype))
+        if key not in self._dev:
+            nodes = self.refel.nodes
+            diff = nodes[:, :, None] - nodes[:, None, :]
+            dist = np.sqrt((diff ** 2).sum(axis=0))
+            min_dr = dist[np.triu_indices(nodes.shape[1], k=1)].min()
+            nvec = np.einsum("erj,fr->efj", self.geometry.rx, self.refel.ref_face_normals)
+            areas = np.linalg.norm(nvec, axis=2) * self.refel.ref_face_areas[None, :]
+            r_d = self.dim * self.refel.ref_volume / areas.sum(axis=1)
+            h = np.repeat((min_dr * r_d)[:, None], self.refel.nnodes, axis=1)
+            self._dev[key] = torch.as_tensor(
+                h, dtype=dtype or torch.float64,
+                device=device if device is not None else self._device)
+        return self._dev[key]
+
     def nodes(self, device=None):
         """Volume node coordinates, a list of d tensors [E, Np] (dcoll.nodes())."""
         import torch

@@ -134,6 +134,40 @@ class PyrometheusMixture(MixtureEOS):
     def internal_energy(self, cv):
         return cv.energy - self.kinetic_energy(cv)
 
+    def _species_cp_r(self, temperature):
+        """NASA-7 c_p,k / R per species, (Ns, ...), the range chosen by T."""
+        import torch
+        m = self._mech
+        t = temperature
+        shape = (-1,) + (1,) * t.ndim
+        lo = torch.as_tensor(m.nasa_low, dtype=t.dtype, device=t.device)
+        hi = torch.as_tensor(m.nasa_high, dtype=t.dtype, device=t.device)
+        sel = t[None] > torch.as_tensor(m.t_mid, dtype=t.dtype, device=t.device).reshape(shape)
+        a = [torch.where(sel, hi[:, j].reshape(shape), lo[:, j].reshape(shape)) for j in range(5)]
+        return a[0] + t * (a[1] + t * (a[2] + t * (a[3] + t * a[4])))
+
+    def heat_capacity_cp(self, cv, temperature):
+        """Mixture c_p per unit mass (mirgecom/eos.py:631-635)."""
+        y = cv.species_mass_fractions
+        w = _wcol(self._mech.molecular_weights, y)
+        return GAS_CONSTANT * (y * self._species_cp_r(temperature) / w).sum(dim=0)
+
+    def heat_capacity_cv(self, cv, temperature):
+        """c_v = c_p - R_mix (mirgecom/eos.py:637-642)."""
+        return self.heat_capacity_cp(cv, temperature) - self.gas_const(cv)
+
+    def gamma(self, cv, temperature):
+        """c_p / (c_p - R_mix) (mirgecom/eos.py:644-650)."""
+        return self.heat_capacity_cp(cv, temperature) / self.heat_capacity_cv(cv, temperature)
+
+    def pressure(self, cv, temperature):
+        """p = rho R_mix T (mirgecom/eos.py:751-761)."""
+        return cv.mass * self.gas_const(cv) * temperature
+
+    def sound_speed(self, cv, temperature):
+        """c = sqrt(gamma p / rho) (mirgecom/eos.py:763-776)."""
+        return (self.gamma(cv, temperature) * self.pressure(cv, temperature) / cv.mass).sqrt()
+
     def fill_struct(self, s: _lib.GasStruct):
         s.eos_kind = _lib.EOS_MIXTURE
         s.niter = self._niter

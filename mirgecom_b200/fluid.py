@@ -50,6 +50,11 @@ class ConservedVars:
         return self.momentum / self.mass
 
     @property
+    def speed(self):
+        """|v| (mirgecom/fluid.py:241-244)."""
+        return (self.velocity ** 2).sum(dim=0).sqrt()
+
+    @property
     def species_mass_fractions(self):
         return self.species_mass / self.mass
 

@@ -102,6 +102,37 @@ class FluidState:
             return self.cv.mass * eos.gas_const(self.cv) * self.temperature
         return eos.pressure(self.cv)
 
+    # dependent and transport variables evaluated on the host side with torch
+    # (mirgecom/gas_model.py:209-286); the operators compute their own copies
+    # inside the kernels
+    @property
+    def speed(self):
+        return self.cv.speed
+
+    @property
+    def speed_of_sound(self):
+        eos = self.gas_model.eos
+        if self.is_mixture:
+            return eos.sound_speed(self.cv, self.temperature)
+        return eos.sound_speed(self.cv)
+
+    @property
+    def wavespeed(self):
+        """|v| + c (mirgecom/gas_model.py:224-226)."""
+        return self.speed + self.speed_of_sound
+
+    @property
+    def viscosity(self):
+        return self.gas_model.transport.viscosity(self.cv, self, self.gas_model.eos)
+
+    @property
+    def thermal_conductivity(self):
+        return self.gas_model.transport.thermal_conductivity(self.cv, self, self.gas_model.eos)
+
+    @property
+    def species_diffusivity(self):
+        return self.gas_model.transport.species_diffusivity(self.cv, self, self.gas_model.eos)
+
 
 def make_fluid_state(cv: ConservedVars, gas_model: GasModel, temperature_seed=None,
                      **kwargs):

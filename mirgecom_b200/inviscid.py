@@ -87,3 +87,15 @@ def flux_kind_of(func):
             f"{func!r} is not a device-supported inviscid numerical flux; use "
             "inviscid_facial_flux_rusanov, _hll or _central")
     return kind
+
+
+def get_inviscid_timestep(dcoll, state, dd=None):
+    """Node-local stable time step of an inviscid fluid, h / (|v| + c)
+    (mirgecom/inviscid.py:379-422), h the characteristic length scale of
+    :meth:`~mirgecom_b200.discretization.Discretization.characteristic_lengthscales`.
+    Returns a tensor shaped like the state's fields (E, Np)."""
+    if dd is not None and dd != "vol":
+        raise TypeError("dd must represent the volume")
+    ws = state.wavespeed
+    h = dcoll.characteristic_lengthscales(device=ws.device, dtype=ws.dtype)
+    return h / ws

@@ -64,6 +64,32 @@ class PowerLawTransport(TransportModel):
                          else np.asarray(species_diffusivity, dtype=np.float64))
         self._lewis = None if lewis is None else np.asarray(lewis, dtype=np.float64)
 
+    # host evaluations (mirgecom/transport.py:255-321); dv is the fluid state
+    # (its temperature), as the reference passes its dependent variables
+    def viscosity(self, cv=None, dv=None, eos=None):
+        """mu = beta T^n."""
+        return self._beta * dv.temperature ** self._n
+
+    def bulk_viscosity(self, cv=None, dv=None, eos=None):
+        return self._alpha * self.viscosity(cv, dv)
+
+    def volume_viscosity(self, cv=None, dv=None, eos=None):
+        return (self._alpha - 2.0 / 3.0) * self.viscosity(cv, dv)
+
+    def thermal_conductivity(self, cv=None, dv=None, eos=None):
+        """kappa = sigma mu c_v."""
+        return self._sigma * self.viscosity(cv, dv) * eos.heat_capacity_cv(cv, dv.temperature)
+
+    def species_diffusivity(self, cv=None, dv=None, eos=None):
+        """Given diffusivities, or sigma mu / (rho Le gamma) from Lewis numbers."""
+        if self._lewis is not None:
+            import torch
+            le = torch.as_tensor(self._lewis, dtype=cv.mass.dtype, device=cv.mass.device)
+            le = le.reshape((-1,) + (1,) * cv.mass.ndim)
+            return (self._sigma * self.viscosity(cv, dv)
+                    / (cv.mass * le * eos.gamma(cv, dv.temperature)))
+        return self._d_alpha
+
     def fill_struct(self, s: _lib.GasStruct, nspecies: int):
         s.transport_kind = _lib.TR_POWERLAW
         s.pl_alpha = self._alpha

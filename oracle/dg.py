@@ -395,3 +395,34 @@ def rk4_step(q, t, dt, rhs):
     k3 = rhs(t + dt / 2, q + dt / 2 * k2)
     k4 = rhs(t + dt, q + dt * k3)
     return q + dt / 6 * (k1 + 2 * k2 + 2 * k3 + k4)
+
+
+# {{{ time-step estimates (mirgecom/inviscid.py:379-422, viscous.py:547-607)
+
+def characteristic_lengthscales(od):
+    """grudge's ``dt_utils.characteristic_lengthscales`` restated (grudge is
+    not installed; Hesthaven & Warburton 2008, sec. 6.4): h = min(dr) r_D with
+    min(dr) the smallest distance between two reference-element nodes and
+    r_D = d V / sum_f F_f the inradius, here from the element's vertices
+    (volume from the vertex Jacobian, face areas from the face vertices)."""
+    nodes = od.refel.nodes
+    n = nodes.shape[1]
+    min_dr = min(float(np.linalg.norm(nodes[:, i] - nodes[:, j]))
+                 for i in range(n) for j in range(i + 1, n))
+    vol = np.abs(od.jac_det) * od.refel.ref_volume
+    areas = od.face_area_ratio * od.refel.face_param_area
+    r_d = od.dim * vol / areas.sum(axis=1)
+    return np.repeat((min_dr * r_d)[:, None], n, axis=1)
+
+
+def inviscid_timestep(od, st):
+    return characteristic_lengthscales(od) / ph.wavespeed(st)
+
+
+def viscous_timestep(od, st):
+    h = characteristic_lengthscales(od)
+    nu = st["mu"] / st["cv"][0] if "mu" in st else 0.0
+    dmax = st["diff"].max(axis=0) if "diff" in st and len(st["diff"]) else 0.0
+    return h / (ph.wavespeed(st) + (nu + dmax) / h)
+
+# }}}
