@@ -33,16 +33,15 @@ def _dot_n(f, normal):
     return (f * normal[None]).sum(dim=1)
 
 
-def _wavespeed(state):
-    v = state.velocity
-    gamma = state.gas_model.eos.gamma()
-    c = (gamma * state.pressure / state.cv.mass).sqrt()
-    return (v * v).sum(dim=0).sqrt() + c
+def _gamma(eos, state):
+    if state.is_mixture:
+        return eos.gamma(state.cv, state.temperature)
+    return eos.gamma()
 
 
 def inviscid_facial_flux_rusanov(state_pair, gas_model=None, normal=None):
     sm, sp = state_pair
-    lam = torch.maximum(_wavespeed(sm), _wavespeed(sp))
+    lam = torch.maximum(sm.wavespeed, sp.wavespeed)
     return num_flux_lfr(_dot_n(inviscid_flux(sm), normal), _dot_n(inviscid_flux(sp), normal),
                         sm.cv.q, sp.cv.q, lam)
 
@@ -60,13 +59,12 @@ def inviscid_facial_flux_hll(state_pair, gas_model=None, normal=None):
     u_int = (sm.velocity * normal).sum(dim=0)
     u_ext = (sp.velocity * normal).sum(dim=0)
     rho_int, rho_ext = sm.cv.mass, sp.cv.mass
-    g = eos.gamma()
-    c_int = (g * p_int / rho_int).sqrt()
-    c_ext = (g * p_ext / rho_ext).sqrt()
+    c_int, c_ext = sm.speed_of_sound, sp.speed_of_sound
     p_star = (0.5 * (p_int + p_ext) + (1. / 8.) * (u_int - u_ext)
               * (rho_int + rho_ext) * (c_int + c_ext))
-    q_int = 1 + (g + 1) / (2 * g) * (p_star / p_int - 1)
-    q_ext = 1 + (g + 1) / (2 * g) * (p_star / p_ext - 1)
+    g_int, g_ext = _gamma(eos, sm), _gamma(eos, sp)
+    q_int = 1 + (g_int + 1) / (2 * g_int) * (p_star / p_int - 1)
+    q_ext = 1 + (g_ext + 1) / (2 * g_ext) * (p_star / p_ext - 1)
     q_int_rt = torch.where(p_star > p_int, q_int, torch.ones_like(q_int)).sqrt()
     q_ext_rt = torch.where(p_star > p_ext, q_ext, torch.ones_like(q_ext)).sqrt()
     s_minus = u_int - c_int * q_int_rt
