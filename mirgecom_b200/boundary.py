@@ -64,8 +64,41 @@ class PrescribedFluidBoundary(FluidBoundary):
         self._bnd_state_func = boundary_state_func
 
     def exterior_state(self, dcoll, dd_bdry, gas_model, state_minus: FluidState, time,
-                       nodes=None) -> FluidState:
+                       nodes=None, normals=None) -> FluidState:
         if self._bnd_state_func is None:
             return state_minus
         return self._bnd_state_func(dcoll=dcoll, dd_bdry=dd_bdry, gas_model=gas_model,
                                     state_minus=state_minus, time=time, nodes=nodes)
+
+
+class AdiabaticSlipBoundary(PrescribedFluidBoundary):
+    """Adiabatic slip wall, inviscid part (mirgecom/boundary.py:1052-1080):
+    the exterior state of the inviscid numerical flux is the interior state
+    with its normal momentum reflected, m+ = m - 2 (m . n) n
+    (``_SlipBoundaryComponent.momentum_plus``, boundary.py:152-153); density,
+    total energy, species and temperature are the interior ones.  On the
+    device it is a prescribed boundary whose exterior state is computed here
+    from the interior trace.  The viscous wall treatment of the reference
+    (``state_bc``, ``grad_cv_bc``, ``grad_temperature_bc``, boundary.py:
+    1082-1143) is not built: ``euler_operator`` accepts this boundary,
+    ``ns_operator`` raises ``NotImplementedError``."""
+
+    device_kind = 1
+    inviscid_only = True
+
+    def __init__(self):
+        self._bnd_state_func = None
+
+    def exterior_state(self, dcoll, dd_bdry, gas_model, state_minus: FluidState, time,
+                       nodes=None, normals=None) -> FluidState:
+        from mirgecom_b200.fluid import ConservedVars
+        if normals is None:
+            raise ValueError("the slip wall needs the boundary normals")
+        d = state_minus.dim
+        q = state_minus.cv.q.clone()
+        n = normals.to(q.dtype)
+        mom = q[2:2 + d]
+        q[2:2 + d] = mom - 2.0 * (mom * n).sum(dim=0) * n
+        return FluidState(ConservedVars(q, d), gas_model,
+                          temperature=state_minus._temperature,
+                          operator_temperature=state_minus.operator_temperature)

@@ -210,8 +210,11 @@ def boundary_exterior(dd, state, gas_model, boundaries, time):
         mask = torch.from_numpy(dcoll.boundary_face_mask(tag)).to(q.device)
         sm = FluidState(ConservedVars(qm[:, mask], state.dim), gas_model,
                         temperature=None if tm is None else tm[mask])
+        nrm = torch.from_numpy(np.ascontiguousarray(
+            dcoll.boundary_normals_numpy()[dcoll.boundary_face_mask(tag)].T)).to(q.device)
         ext = bdry.exterior_state(dcoll, tag, gas_model, sm, time,
-                                  nodes=dcoll.boundary_nodes(tag, q.device))
+                                  nodes=dcoll.boundary_nodes(tag, q.device),
+                                  normals=nrm[:, :, None])
         bext[:nc, mask] = ext.cv.q.to(q.dtype)
         if state.is_mixture:
             bext[nc, mask] = ext.temperature.to(q.dtype)
@@ -275,12 +278,22 @@ def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
     return rhs
 
 
+def _refuse_inviscid_only(boundaries):
+    """The viscous treatment of a wall that only the inviscid operator
+    supports (the slip wall) is not built."""
+    bad = [t for t, b in boundaries.items() if getattr(b, "inviscid_only", False)]
+    if bad:
+        raise NotImplementedError(
+            f"boundaries {bad}: only their inviscid treatment is built (euler_operator)")
+
+
 def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
            source_temperature=None, grad_out=None, events=None):
     """Gradient + divergence passes.  *events* (3 or 4 CUDA events) are
     recorded before the gradient pass, between the passes, (with 4: between
     the node-flux and surface kernels of the split divergence) and after the
     divergence."""
+    _refuse_inviscid_only(boundaries)
     q = state.cv.q
     _lib.require_cuda(q)
     q = q.contiguous()
@@ -359,6 +372,7 @@ def rk4_stage(q0, k, acc, qout, stage, dt, qout_lo=None):
 
 def ns_gradients(dcoll, state, gas_model, boundaries, time):
     """Gradient pass only: [Nc+1, dim, E, Np] (workspace tensor)."""
+    _refuse_inviscid_only(boundaries)
     q = state.cv.q
     _lib.require_cuda(q)
     q = q.contiguous()

@@ -213,6 +213,13 @@ class PrescribedBoundary:
         self.func = func
 
 
+class AdiabaticSlipBoundary:
+    """mirgecom/boundary.py:1052-1080 (state_plus) with the slip component's
+    momentum_plus (boundary.py:152-153): for the inviscid flux the exterior
+    state is the interior one with its normal momentum reflected, m+ = m -
+    2 (m . n) n.  The viscous (Mengaldo) wall treatment is not restated."""
+
+
 def _normalize_boundaries(boundaries):
     return boundaries or {}
 
@@ -258,6 +265,12 @@ def make_operator_fluid_states(disc, state, gas, transport, boundaries, time):
         sm = ph.make_fluid_state(qb, gas, transport, dim, temperature_seed=tb)
         if isinstance(bdry, DummyBoundary):
             sp = sm
+        elif isinstance(bdry, AdiabaticSlipBoundary):
+            nb = _bnormals(disc)
+            qe = qb.copy()
+            mom = qe[2:2 + dim]
+            qe[2:2 + dim] = mom - 2.0 * np.sum(mom * nb, axis=0) * nb
+            sp = ph.make_fluid_state(qe, gas, transport, dim, temperature_seed=tb)
         else:
             xb = disc.nodes[:, be[:, None], fnodes]
             ext = bdry.func(xb, time)
