@@ -83,6 +83,45 @@ def test_static_vortex_rhs_converges(kind, order):
     assert _eoc(hs, errs) >= order - 0.7, (hs, errs)
 
 
+def _shear_flow_np(x, flow, trans, mu=0.01, gamma=1.5):
+    """Hesthaven & Warburton sec. 7.5.3 shear flow (the reference's
+    initializers.py:1421-1520): rho = 1, v_flow = x_trans^2, other velocity
+    components 0, rho E = (2 mu x_flow + 10) / (gamma - 1) + x_trans^4 / 2 --
+    a steady solution of the compressible Navier-Stokes equations with zero
+    heat conduction."""
+    dim = x.shape[0]
+    q = np.zeros((dim + 2,) + x.shape[1:])
+    q[0] = 1.0
+    q[2 + flow] = x[trans] ** 2
+    q[1] = (2 * mu * x[flow] + 10) / (gamma - 1) + x[trans] ** 4 / 2
+    return q
+
+
+@pytest.mark.parametrize("kind,dim,order,flow", [("simplex", 2, 2, 0), ("simplex", 2, 3, 1),
+                                                 ("hypercube", 2, 2, 0),
+                                                 ("simplex", 3, 2, 2)])
+def test_shear_flow_ns_rhs_converges(kind, dim, order, flow):
+    """test/test_navierstokes.py:615-713: the NS RHS of the exact shear flow,
+    with exact prescribed boundary states, vanishes: continuity exactly, the
+    energy equation at order >= p - 0.5 (or below 1e-8)."""
+    trans = (flow + 1) % dim
+    gas = oph.IdealGas(gamma=1.5, gas_const=287.0)
+    tr = oph.SimpleTransportParams(viscosity=0.01, thermal_conductivity=0.0)
+    base = 4 if dim == 2 else 2
+    hs, errs, mass = [], [], []
+    for n in (1, 2, 4):
+        _, od = make_disc(kind, dim, base * n, order, (0.0,) * dim, (1.0,) * dim, False)
+        q = _shear_flow_np(od.nodes, flow, trans)
+        st = oph.make_fluid_state(q, gas, tr, dim)
+        bnd = {"all": odg.PrescribedBoundary(lambda x, t: _shear_flow_np(x, flow, trans))}
+        rhs = odg.ns_operator(od, st, gas, tr, bnd)
+        hs.append(1.0 / (base * n))
+        errs.append(np.sqrt(np.mean(rhs[1] ** 2)))
+        mass.append(np.abs(rhs[0]).max())
+    assert max(mass) < 1e-10, mass
+    assert _eoc(hs, errs) >= order - 0.5 or max(errs) < 1e-8, (hs, errs)
+
+
 @pytest.mark.parametrize("dim,order", [(2, 1), (2, 3), (3, 2)])
 def test_gradient_exact_for_polynomials(dim, order):
     """test/test_operators.py:257-417 (coordinate functions of degree <= p):
