@@ -183,6 +183,46 @@ def test_manufactured_ns_rhs_converges(kind, order):
     assert _eoc(hs, errs) >= order - 1.3, (hs, errs)
 
 
+def _multilump_np(x, nspecies, v0, rho0=2.0, p0=1.0, sigma=1.0, gamma=1.4):
+    """Passive species lumps advected by a uniform flow (the reference's
+    MulticomponentLump, initializers.py:594-752, with its defaults): rho = rho0,
+    v = (v0, 0, ..), p = p0, rho Y_i = rho0 (1 + exp(-r^2 / (2 sigma^2))).
+    Returns the state and the exact Euler RHS (only the species move:
+    d(rho Y_i)/dt = -v . grad(rho Y_i))."""
+    dim = x.shape[0]
+    vel = np.zeros(dim)
+    vel[0] = v0
+    q = np.zeros((dim + 2 + nspecies,) + x.shape[1:])
+    q[0] = rho0
+    q[1] = p0 / (gamma - 1) + 0.5 * rho0 * v0 ** 2
+    q[2] = rho0 * v0
+    r2 = np.sum(x * x, axis=0) / sigma ** 2
+    lump = np.exp(-0.5 * r2)
+    rhs = np.zeros_like(q)
+    for i in range(nspecies):
+        q[2 + dim + i] = rho0 * (1.0 + lump)
+        rhs[2 + dim + i] = rho0 * lump * np.tensordot(vel, x, axes=(0, 0)) / sigma ** 2
+    return q, rhs
+
+
+@pytest.mark.parametrize("kind,dim,order", [("simplex", 2, 1), ("simplex", 2, 3),
+                                            ("simplex", 3, 2), ("hypercube", 2, 2)])
+@pytest.mark.parametrize("flux", ["rusanov", "hll"])
+def test_multilump_euler_rhs_converges(kind, dim, order, flux):
+    """test/test_euler.py:577-665: the Euler RHS of advected species lumps
+    converges to the exact one at order >= p - 0.5."""
+    hs, errs = [], []
+    for n in (4, 8, 12):
+        _, od = make_disc(kind, dim, n, order, (-1.0,) * dim, (1.0,) * dim, False)
+        q, exact = _multilump_np(od.nodes, 3, 1.0)
+        st = oph.make_fluid_state(q, oph.IdealGas(), None, dim)
+        bnd = {"all": odg.PrescribedBoundary(lambda xx, t: _multilump_np(xx, 3, 1.0)[0])}
+        rhs = odg.euler_operator(od, st, oph.IdealGas(), bnd, flux=flux)
+        hs.append(1.0 / n)
+        errs.append(np.abs(rhs - exact).max())
+    assert _eoc(hs, errs) >= order - 0.5 or max(errs) < 1e-8, (hs, errs)
+
+
 @pytest.mark.parametrize("dim,order", [(2, 1), (2, 3), (3, 2)])
 def test_gradient_exact_for_polynomials(dim, order):
     """test/test_operators.py:257-417 (coordinate functions of degree <= p):
