@@ -44,3 +44,53 @@ def test_invalid_arguments_rejected_without_gpu():
     lib = _lib.load()
     assert lib.mgc_euler_rhs(None, None, None, None, None, 0, None, None, None) == -1
     assert lib.mgc_rk4_stage(-1, None, None, None, None, None, 0, 0.1, None) == -1
+
+
+_QUERIES = {"mgc_version", "mgc_supports", "mgc_supports_hex", "mgc_mlp_nparams",
+            "mgc_rhs_split_workspace_bytes", "mgc_mlp_train_workspace_bytes",
+            "mgc_ns_operator_noalloc_capacity"}
+
+
+def _null_call_script():
+    """Python source that calls every non-query entry point with null
+    pointers, zero dimensions and negative sizes and prints the codes."""
+    return r'''
+import ctypes as C, json, sys
+sys.path.insert(0, %r)
+from mirgecom_b200 import _lib
+lib = _lib.load()
+out = {}
+for name, (args, res) in _lib._SIGNATURES.items():
+    if name in %r:
+        continue
+    vals = []
+    for a in args:
+        if a is C.c_void_p:
+            vals.append(None)
+        elif a is C.c_int64:
+            vals.append(-1)
+        elif a in (C.c_float, C.c_double):
+            vals.append(0.0)
+        elif a is C.c_size_t:
+            vals.append(0)
+        else:
+            vals.append(0)
+    out[name] = getattr(lib, name)(*vals)
+print(json.dumps(out))
+''' % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))), sorted(_QUERIES))
+
+
+def test_every_entry_point_rejects_null_arguments():
+    """Null pointers, zero dimensions and negative sizes come back as a
+    negative code from every entry point, before any device work, in a child
+    process (so that a crash would fail this test, not the run)."""
+    import json
+    import subprocess
+    import sys
+    res = subprocess.run([sys.executable, "-c", _null_call_script()], capture_output=True,
+                         text=True, timeout=120)
+    assert res.returncode == 0, res.stderr[-2000:]
+    codes = json.loads(res.stdout.strip().splitlines()[-1])
+    assert set(codes) == set(_lib.exported_symbols()) - _QUERIES
+    bad = {k: v for k, v in codes.items() if v >= 0}
+    assert not bad, bad
