@@ -120,7 +120,7 @@ def build_workload(name, device):
 
 
 KERNEL_NAMES = {"state": "k_mixture_state*", "grad": "k_grad", "node_flux": "k_node_flux",
-                "surface": "k_surface"}
+                "surface": "k_surface", "volume": "k_volume", "face": "k_face"}
 
 
 def algorithmic_bytes(dcoll, nc, s=8, mixture=False):
@@ -140,7 +140,19 @@ def algorithmic_bytes(dcoll, nc, s=8, mixture=False):
     t_in = 1 if mixture else 0
     ns = nc - d - 2
     fw = -(-(nc * d + 4) // 4) * 4
+    nfn = dcoll.nfaces * dcoll.nface_nodes
+    tw = -(-(nc + 4) // 4) * 4
+    ne = dcoll.nelements
     out = {
+        # volume: read q [+ T (+ source T on the float64 path)], write the
+        # volume part of the rhs, the face-node records (Nf Nfp x TW per
+        # element) and the node-0 shifts (Nf Nc per element)
+        "volume": nn * (nc + t_in * (2 if s == 8 else 1) + nc) * s
+                  + ne * (nfn * tw + dcoll.nfaces * nc) * s + geo,
+        # face: read the own records and the node-0 shifts, q at the own face
+        # nodes, the rhs, write the rhs (the neighbours' records and q come
+        # from L2 when the element order keeps neighbours close)
+        "face": ne * (nfn * tw + dcoll.nfaces * nc) * s + nn * (nc + 2 * nc) * s + geo,
         "grad": nn * (nc + t_in + (nc + 1) * d) * s + geo,
         "node_flux": nn * (nc + (nc + 1) * d + 2 * t_in + fw + (ns if mixture else 0)) * s,
         "surface": nn * (fw + nc + (ns if mixture else 0) + nc) * s + geo,
@@ -365,23 +377,31 @@ def _rhs_call(dcoll, gas, q, tseed, events=None):
 
 def _time_form(dcoll, gas, q, tseed, steps, warmup, flush, stream):
     import torch
+
+    from mirgecom_b200 import runtime
+    vf = runtime._path(dcoll) == "volume_face"
+    nev = 4 if vf else 5
     for _ in range(warmup):
         _rhs_call(dcoll, gas, q, tseed)
     torch.cuda.synchronize()
     evs = []
     for i in range(steps):
         flush.fill_(float(i))
-        # start | state | grad | node_flux | surface
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        # start | state | volume | face    or    start | state | grad | node_flux | surface
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(nev)]
         _rhs_call(dcoll, gas, q, tseed, events=ev)
         evs.append(ev)
     torch.cuda.synchronize()
-    step_ms = [e[0].elapsed_time(e[4]) for e in evs]
+    step_ms = [e[0].elapsed_time(e[-1]) for e in evs]
 
     def mean(i, j):
         return float(np.mean([e[i].elapsed_time(e[j]) for e in evs]))
-    kern = {"state": mean(0, 1), "grad": mean(1, 2), "node_flux": mean(2, 3),
-            "surface": mean(3, 4), "rhs": mean(2, 4)}
+    if vf:
+        kern = {"state": mean(0, 1), "volume": mean(1, 2), "face": mean(2, 3),
+                "rhs": mean(1, 3)}
+    else:
+        kern = {"state": mean(0, 1), "grad": mean(1, 2), "node_flux": mean(2, 3),
+                "surface": mean(3, 4), "rhs": mean(2, 4)}
     return float(np.sum(step_ms)), kern
 
 
@@ -467,23 +487,49 @@ def _end_of_run(dcoll, gas, q64, nsteps, n_axis):
             "wall_s": time.perf_counter() - t0}
 
 
-def _end_of_run_mixture(dcoll, gas, gas_head, q64, t64, nsteps, dt=5e-9):
+def chemical_time_scale(dcoll, gas, q64, t64):
+    """Smallest chemical time scale of the state: min over nodes and species
+    with Y_k > 1e-3 of rho Y_k / |W_k omega_k|, the sources taken as the
+    difference of the float64 right-hand sides with and without them."""
+    import torch
+
+    from mirgecom_b200 import runtime
+    from mirgecom_b200.fluid import ConservedVars
+    from mirgecom_b200.gas_model import make_fluid_state
+    st = make_fluid_state(ConservedVars(q64, 3), gas, temperature_seed=t64)
+    with_src, _ = runtime.ns_rhs(dcoll, st, gas, {}, 0.0, 0, source_temperature=st.temperature)
+    without, _ = runtime.ns_rhs(dcoll, st, gas, {}, 0.0, 0)
+    src = (with_src - without)[5:]
+    rhoy = q64[5:]
+    mask = (rhoy / q64[0]) > 1e-3
+    tau = rhoy.abs() / src.abs().clamp_min(1e-300)
+    return float(torch.where(mask, tau, torch.full_like(tau, float("inf"))).min())
+
+
+def _end_of_run_mixture(dcoll, gas, gas_head, q64, t64, nsteps, dt=None):
     """*nsteps* RK4 steps of the reacting workload in the float64 form and in
     the headline form (mixed precision + learned guess: float64 RK
     accumulation, float32 right-hand sides) from the same state, species
     sources on, each form's temperature seeded with its own previous
-    temperature.  The synthetic states ignite: the difference between the
-    two forms grows with the simulated time as the chemistry amplifies
-    float32-level differences (measured on 40^3 p2 tets: largest field
-    difference 2e-7 after 2.5e-7 s, 5e-5 after 1e-6 s), so the default run is
-    40 steps of 5e-9 s.  Returns the per-field relative L2 difference at the
-    end and the temperatures' difference."""
+    temperature.  dt (default) resolves the chemistry: the smallest chemical
+    time scale of the initial state over 64.  The synthetic states ignite,
+    and over longer horizons the flow itself amplifies float32-level
+    differences (on the float64 oracle alone a 6e-8 perturbation of the
+    initial state grows to 4.5e-6 over 200 steps of 5e-9 s, tests/
+    end_of_run_sensitivity.py).  Returns the per-field relative L2 difference
+    at the end and the temperatures' difference."""
     import torch
 
     from mirgecom_b200.fluid import ConservedVars
     from mirgecom_b200.gas_model import make_fluid_state
     from mirgecom_b200.integrators import rk4_step, rk4_step_mixed
     from mirgecom_b200.navierstokes import ns_operator
+
+    tau = chemical_time_scale(dcoll, gas, q64, t64)
+    dt_rule = "given"
+    if dt is None:
+        dt = tau / 64
+        dt_rule = "smallest chemical time scale / 64"
 
     def factory(g, box):
         def rhs(t, cv):
@@ -513,13 +559,74 @@ def _end_of_run_mixture(dcoll, gas, gas_head, q64, t64, nsteps, dt=5e-9):
                 for c in range(y.shape[0])]
     ta, tb = b32[0].double().cpu().numpy(), b64[0].cpu().numpy()
     species = list(gas.eos.mechanism.species)
-    return {"steps": nsteps, "dt": dt, "t_final": nsteps * dt,
+    return {"steps": nsteps, "dt": dt, "dt_rule": dt_rule, "tau_chem_min": tau,
+            "t_final": nsteps * dt,
             "form": "mixed_learned vs plain_fp64",
             "fields": ["mass", "energy", "momentum_x", "momentum_y", "momentum_z"] +
                       [f"rho_{sp}" for sp in species],
             "mixed_vs_fp64_rel_l2": rel(a, b), "fp64_change_rel_l2": rel(b, q0),
             "temperature_rel_l2": float(np.linalg.norm(ta - tb) / np.linalg.norm(tb)),
             "wall_s": time.perf_counter() - t0}
+
+
+def run_vortex(args):
+    """The 2-D vortex configuration run to t = 1 (200 RK4 steps of 0.005)
+    through the library's driver (mirgecom_b200.vortex) on the GPU, and the
+    float64 oracle's same run on one host core: wall times, L2 errors
+    against the exact solution, and the largest per-field difference of the
+    two end states."""
+    import torch
+
+    from mirgecom_b200 import vortex
+    rank, world, local = _dist_env()
+    if rank != 0:
+        return
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    vortex.run(device=dev, nsteps=2)            # warm-up: uploads, kernel set-up
+    res = vortex.run(device=dev)
+    q_gpu = res["q"].cpu().numpy()
+    from mirgecom_b200.discretization import Discretization
+    from mirgecom_b200.mesh import generate_box_mesh
+    from oracle import dg as odg
+    from oracle import physics as oph
+    c = vortex.CASE
+    mesh = generate_box_mesh(c["a"], c["b"], (c["nel"], c["nel"]))
+    d = Discretization(mesh, c["order"])
+    od = odg.OracleDisc(mesh, d.refel)
+    init = vortex.Vortex2D(beta=c["beta"], center=c["center"], velocity=c["velocity"])
+
+    def exact(x, t):
+        return init([torch.from_numpy(x[i]) for i in range(2)], time=t).q.numpy()
+
+    obnds = {"all": odg.PrescribedBoundary(exact)}
+
+    def orhs(t, qq):
+        return odg.euler_operator(od, oph.make_fluid_state(qq, oph.IdealGas(), None, 2),
+                                  oph.IdealGas(), obnds, time=t)
+
+    q = exact(od.nodes, 0.0)
+    t0 = time.perf_counter()
+    for i in range(res["steps"]):
+        q = odg.rk4_step(q, i * c["dt"], c["dt"], orhs)
+    cpu_wall = time.perf_counter() - t0
+    r = q - exact(od.nodes, res["t"])
+    det = np.abs(d.geometry.det)
+    cpu_err = [float(np.sqrt(np.sum(det * np.einsum("ei,ij,ej->e", r[k], d.refel.mass, r[k]))))
+               for k in range(4)]
+    diff = [float(np.linalg.norm(q_gpu[k] - q[k]) / np.linalg.norm(q[k])) for k in range(4)]
+    nrhs = 4 * res["steps"]
+    fields = ["mass", "energy", "momentum_x", "momentum_y"]
+    print(json.dumps({
+        "case": "vortex2d_p3", "desc": "2-D Euler isentropic vortex, [0,10]x[-5,5], 16x16x2 "
+        "triangles, order 3, beta 5 at (5,0), velocity (1,0), exact prescribed boundaries, "
+        "Rusanov, RK4 dt 0.005 to t = 1", "steps": res["steps"], "t_final": res["t"],
+        "gpu": {"wall_s": res["wall_s"], "dof_rhs_per_s": res["dof"] * nrhs / res["wall_s"],
+                "l2_error_vs_exact": dict(zip(fields, res["l2_error"]))},
+        "cpu_oracle": {"wall_s": cpu_wall, "cores": 1, "dof_rhs_per_s":
+                       res["dof"] * nrhs / cpu_wall,
+                       "l2_error_vs_exact": dict(zip(fields, cpu_err))},
+        "end_state_rel_l2_gpu_vs_oracle": dict(zip(fields, diff))}), flush=True)
 
 
 def run_ours(args):
@@ -644,6 +751,10 @@ def _run_ours(args):
     q_host = hq.cpu().pin_memory()
     out_host = [torch.empty_like(q_host).pin_memory() for _ in range(2)]
     qd = [torch.empty_like(hq) for _ in range(2)]
+    # a driver holds the step-start temperature on the host with the state
+    # and uploads it with q (mixtures)
+    t_host = ht.cpu().pin_memory() if ht is not None else None
+    td = [torch.empty_like(ht) for _ in range(2)] if ht is not None else [None, None]
     h2d, d2h = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
 
     def pipelined(nsteps):
@@ -657,10 +768,12 @@ def _run_ours(args):
                 h2d.wait_event(read_done[b])
             with torch.cuda.stream(h2d):
                 qd[b].copy_(q_host, non_blocking=True)
+                if t_host is not None:
+                    td[b].copy_(t_host, non_blocking=True)
             loaded = torch.cuda.Event()
             loaded.record(h2d)
             stream.wait_event(loaded)
-            rhs = _rhs_call(dcoll, hgas, qd[b], ht)
+            rhs = _rhs_call(dcoll, hgas, qd[b], td[b])
             read_done[b] = torch.cuda.Event()
             read_done[b].record(stream)
             d2h.wait_event(read_done[b])
@@ -701,7 +814,7 @@ def _run_ours(args):
     # this library's kernels per step: temperature (mixtures), gradient, and
     # the divergence pass (node flux + surface on the split path)
     from mirgecom_b200 import runtime as _rt
-    per_step = (1 if mixture else 0) + 1 + (2 if _rt.SPLIT_RHS else 1)
+    per_step = (1 if mixture else 0) + (2 if _rt._path(dcoll) == "volume_face" else 3)
     line = {
         "metric": "DOF-RHS evals/s", "value": values[head], "unit": "DOF-RHS/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -721,8 +834,10 @@ def _run_ours(args):
         "kernels_ms": k32,
         "learned_guess": learned,
         "e2e": {"value": e2e_value, "unit": "DOF-RHS/s",
-                "h2d_bytes_per_step": hq.numel() * 4, "d2h_bytes_per_step": hq.numel() * 4,
-                "schedule": "pipelined: host-to-device copy of step i, RHS of step i and "
+                "h2d_bytes_per_step": hq.numel() * 4 + (ht.numel() * 4 if ht is not None else 0),
+                "d2h_bytes_per_step": hq.numel() * 4,
+                "schedule": "pipelined: host-to-device copy of step i (state and, for "
+                            "mixtures, the step-start temperature), RHS of step i and "
                             "device-to-host copy of step i-1 on separate streams; pinned host "
                             "buffers; inputs larger than L2"},
         "gpu_launches": per_step * args.steps,
@@ -753,18 +868,24 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--end-of-run", type=int, default=40,
+    ap.add_argument("--end-of-run", type=int, default=200,
                     help="after timing, run this many RK4 steps in the float64 and the "
                          "headline mixed form from the same state and report their "
                          "per-field difference (0: skip)")
-    ap.add_argument("--end-of-run-dt", type=float, default=5e-9,
-                    help="time step of the reacting end-of-run comparison (s)")
+    ap.add_argument("--end-of-run-dt", type=float, default=None,
+                    help="time step of the reacting end-of-run comparison (s); default: "
+                         "the state's smallest chemical time scale / 64")
+    ap.add_argument("--vortex-run", action="store_true",
+                    help="run the 2-D vortex configuration to t = 1 on the GPU and with the "
+                         "float64 oracle on one host core, and report both")
     ap.add_argument("--profile", action="store_true",
                     help="time the plain and mixed forms only (no network training, "
                          "end-to-end or CPU legs): the command profiled with ncu")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         run_reference(args)
+    elif args.vortex_run:
+        run_vortex(args)
     else:
         run_ours(args)
 

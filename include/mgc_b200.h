@@ -105,6 +105,8 @@ typedef struct {
   const uint8_t* perm;
   const int8_t* bkind;
   const float* rx32;        /* float32 copy of rx, for the *_f32 entry points */
+  const uint8_t* fslot;     /* [nperm][Nfp] neighbour face slot fn*Nfp + m' of own face
+                               node m (mgc_operator*; may be NULL for the others) */
 } mgc_mesh_t;
 
 /* Library version and the list of supported (dim, order) pairs. */
@@ -141,10 +143,13 @@ int mgc_set_mechanism(const mgc_mechanism_t* mech_host);
 
 /* Mixture temperature (mirgecom/eos.py:777-803 -> thermochemistry.py:126-167):
  * t1 = Newton(e, Y; t_seed), t2 = Newton(e, Y; t1) (t2 may be NULL).
- * nnodes = E*Np. */
+ * nnodes = E*Np.  A node whose solve has not converged (t2, or one further
+ * Newton step when t2 is NULL, moves by more than 1e-6 of t1) or whose
+ * temperature is not positive and finite sets MGC_ST_NEWTON_MISS in *status
+ * (may be NULL); the reference leaves this to its drivers' health checks. */
 int mgc_mixture_temperature(int dim, const mgc_gas_t* gas, int64_t nnodes,
                             const double* q, const double* t_seed, double* t1,
-                            double* t2, void* stream);
+                            double* t2, int32_t* status, void* stream);
 
 /* euler_operator (mirgecom/euler.py:313-416), non-ESDG branch. t_op is the
  * operator temperature for mixtures (NULL for the ideal gas). */
@@ -235,6 +240,33 @@ int mgc_rhs_split_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas,
                       void* workspace, size_t workspace_bytes, int32_t* status, void* stream,
                       void* mid_event);
 
+/* ---- euler_operator (viscous = 0; mirgecom/euler.py:313-416, non-ESDG
+ * branch) or ns_operator (viscous = 1; mirgecom/navierstokes.py:350-575,
+ * with return_gradients when grad_out is non-NULL) in one call on
+ * simplicial meshes: a volume kernel (BR1 gradients kept on chip, pointwise
+ * fluxes and sources, face-node flux records, the volume part of the weak
+ * divergence) and a face kernel (numerical face fluxes from the records of
+ * both sides, lift).  t_op: operator temperature (mixtures); t_src: the
+ * temperature of the species sources (add_sources != 0); bext: prescribed
+ * exterior states [Nc+1][nbf][Nfp] (may be NULL when no boundary face is
+ * prescribed); grad_out: optional [Nc+1][dim][E][Np] gradients.  The mesh
+ * needs fslot.  workspace: 256-byte aligned, at least
+ * mgc_operator_workspace_bytes(mesh, gas, single_precision) bytes (face-node
+ * records [E][Nf][Nfp][round_up(Nc+4, 4)], node-0 fluxes [E][Nf][Nc],
+ * boundary records).  mid_event: a cudaEvent_t recorded between the two
+ * kernels, or NULL.  Hexahedral meshes return MGC_E_UNSUPPORTED (use
+ * mgc_ns_grad* + mgc_rhs_split*). ---- */
+size_t mgc_operator_workspace_bytes(const mgc_mesh_t* mesh, const mgc_gas_t* gas,
+                                    int single_precision);
+int mgc_operator(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
+                 const double* t_op, const double* t_src, const double* bext, int flux_kind,
+                 int add_sources, double* rhs, double* grad_out, void* workspace,
+                 size_t workspace_bytes, int32_t* status, void* stream, void* mid_event);
+int mgc_operator_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
+                     const float* t_op, const float* t_src, const float* bext, int flux_kind,
+                     int add_sources, float* rhs, float* grad_out, void* workspace,
+                     size_t workspace_bytes, int32_t* status, void* stream, void* mid_event);
+
 /* ---- learned initial guess of the mixture temperature (no counterpart in
  * the reference, whose Newton solve always starts from the seed): an
  * 8 -> 64 -> 64 -> 1 tanh MLP, bf16 tensor-core matrix products with float32
@@ -286,6 +318,17 @@ int mgc_mlp_train_grad(int64_t n, const float* x, const float* target, const mgc
 int mgc_mlp_adam(const mgc_mlp_t* w, const float* grad, float* m, float* v, float lr,
                  float beta1, float beta2, float eps, int step, void* stream);
 
+/* ---- FP64 throughput probes (the float64 path's compute roofline).
+ * No counterpart in the reference (a measurement aid).  kind 0 runs
+ * independent fma.rn.f64 chains (the FP64 FMA pipe), kind 1 independent
+ * mma.m8n8k4.f64 chains (the float64 tensor cores) over nblocks x threads
+ * (threads <= 256, a multiple of 32) for iters rounds; sink receives
+ * nblocks*threads doubles.  mgc_fp64_probe_flops gives the flops one launch
+ * performs, for the caller's event timing. */
+double mgc_fp64_probe_flops(int kind, int nblocks, int threads, int iters);
+int mgc_fp64_probe(int kind, int nblocks, int threads, int iters, double* sink,
+                   void* stream);
+
 /* ---- Navier-Stokes right-hand side without device allocation.
  * No counterpart in the reference: it exists for callers that cannot
  * allocate device memory -- a solver that owns all device memory through
@@ -297,8 +340,10 @@ int mgc_mlp_adam(const mgc_mlp_t* w, const float* grad, float* m, float* v, floa
  * buffer ((Nc+1)*dim*E*Np doubles) exceeds it return MGC_E_TOO_LARGE.
  * All calls share that array: calls overlapping on the GPU race and must be
  * serialised by the caller.  The first call on a device looks up the
- * array's device address; make it before any stream capture.  Arguments
- * and results are those of mgc_ns_rhs. ---- */
+ * array's device address; make it before any stream capture.  That address
+ * is kept for the life of the process and does not survive cudaDeviceReset
+ * (or any other teardown of the device's primary context): do not call this
+ * entry point after one.  Arguments and results are those of mgc_ns_rhs. ---- */
 size_t mgc_ns_operator_noalloc_capacity(void);
 
 int mgc_ns_operator_noalloc(const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,

@@ -63,7 +63,7 @@ class MeshStruct(C.Structure):
         ("dim", C.c_int32), ("order", C.c_int32), ("nelem", C.c_int32),
         ("nbf", C.c_int32), ("nperm", C.c_int32), ("elem_kind", C.c_int32),
         ("rx", C.c_void_p), ("conn", C.c_void_p), ("perm", C.c_void_p),
-        ("bkind", C.c_void_p), ("rx32", C.c_void_p),
+        ("bkind", C.c_void_p), ("rx32", C.c_void_p), ("fslot", C.c_void_p),
     ]
 
 
@@ -84,7 +84,7 @@ _SIGNATURES = {
     "mgc_set_mechanism": ([_P], C.c_int),
     "mgc_supports_hex": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
     "mgc_upload_hex_operators": ([C.c_int, C.c_int, _P, _P, C.c_double], C.c_int),
-    "mgc_mixture_temperature": ([C.c_int, _P, C.c_int64, _P, _P, _P, _P, _P], C.c_int),
+    "mgc_mixture_temperature": ([C.c_int, _P, C.c_int64, _P, _P, _P, _P, _P, _P], C.c_int),
     "mgc_euler_rhs": ([_P, _P, _P, _P, _P, C.c_int, _P, _P, _P], C.c_int),
     "mgc_ns_grad": ([_P, _P, _P, _P, _P, _P, _P, _P], C.c_int),
     "mgc_ns_rhs": ([_P, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P], C.c_int),
@@ -112,6 +112,13 @@ _SIGNATURES = {
     "mgc_ns_operator_noalloc_capacity": ([], C.c_size_t),
     "mgc_ns_operator_noalloc": (
         [_P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P], C.c_int),
+    "mgc_operator_workspace_bytes": ([_P, _P, C.c_int], C.c_size_t),
+    "mgc_operator": ([C.c_int, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P,
+                      C.c_size_t, _P, _P, _P], C.c_int),
+    "mgc_operator_f32": ([C.c_int, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P,
+                          C.c_size_t, _P, _P, _P], C.c_int),
+    "mgc_fp64_probe_flops": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_double),
+    "mgc_fp64_probe": ([C.c_int, C.c_int, C.c_int, C.c_int, _P, _P], C.c_int),
 }
 
 _lib = None

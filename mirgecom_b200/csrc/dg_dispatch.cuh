@@ -7,6 +7,7 @@
 #include <cstring>
 
 #include "dg_kernels.cuh"
+#include "dg_volume.cuh"
 #include "../../include/mgc_b200.h"
 
 namespace mgc {
@@ -147,6 +148,46 @@ struct Launch {
   static size_t split_workspace_bytes(int64_t nelem) {
     return ((size_t)nelem * C::NP * C::FW + (size_t)NS * nelem * C::NP) * sizeof(R) + 256;
   }
+  // volume kernel then face kernel (dg_volume.cuh)
+  template <bool VISC>
+  static int vol_face(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
+    using V = VCfg<R, DIM, ORDER, NS, MIX>;
+    const size_t smem1 = V::vol_bytes(V::EPB, a.nperm);
+    auto k1 = k_volume<R, DIM, ORDER, NS, MIX, VISC>;
+    int rc = prepare_kernel(k1, smem1);
+    if (rc) return rc;
+    int nblk = 0;
+    rc = persistent_grid(k1, V::NT, smem1, (a.nelem + V::EPB - 1) / V::EPB, &nblk);
+    if (rc) return rc;
+    k1<<<nblk, V::NT, smem1, s>>>(a, g);
+    if (cudaGetLastError() != cudaSuccess) return MGC_E_CUDA;
+    if (a.mid_event && cudaEventRecord(static_cast<cudaEvent_t>(a.mid_event), s) != cudaSuccess)
+      return MGC_E_CUDA;
+    const size_t smem2 = V::face_bytes(a.nperm);
+    auto k2 = k_face<R, DIM, ORDER, NS, MIX, VISC>;
+    rc = prepare_kernel(k2, smem2);
+    if (rc) return rc;
+    rc = persistent_grid(k2, V::NT2, smem2, (a.nelem + V::EPB2 - 1) / V::EPB2, &nblk);
+    if (rc) return rc;
+    k2<<<nblk, V::NT2, smem2, s>>>(a, g);
+    return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+  }
+  // workspace of vol_face: face-node records, node-0 shifts, boundary
+  // records, boundary plus states, each 256-byte aligned
+  static size_t vol_workspace_parts(int64_t nelem, int64_t nbf, size_t* off_s0,
+                                    size_t* off_btrace, size_t* off_bplus) {
+    using V = VCfg<R, DIM, ORDER, NS, MIX>;
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t nb = (size_t)(nbf > 0 ? nbf : 1);
+    const size_t tr = al((size_t)nelem * V::NFN * V::TW * sizeof(R));
+    const size_t s0 = al((size_t)nelem * V::NF * V::NC * sizeof(R));
+    const size_t bt = al(nb * V::NFP * V::TW * sizeof(R));
+    const size_t bp = al(nb * V::NFP * V::NC * sizeof(R));
+    if (off_s0) *off_s0 = tr;
+    if (off_btrace) *off_btrace = tr + s0;
+    if (off_bplus) *off_bplus = tr + s0 + bt;
+    return tr + s0 + bt + bp;
+  }
   template <bool VISC>
   static int rhs(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
     const size_t smem = C::smem_rhs(a.nperm);
@@ -170,7 +211,9 @@ inline int dispatch_order(int op, int ns, bool mix, const DGArgs<R>& a, const Ga
     if (op == 1) return L::template rhs<false>(a, g, s);                 \
     if (op == 2) return L::template rhs<true>(a, g, s);                  \
     if (op == 3) return L::template rhs_split<false>(a, g, s);           \
-    return L::template rhs_split<true>(a, g, s);                         \
+    if (op == 4) return L::template rhs_split<true>(a, g, s);            \
+    if (op == 5) return L::template vol_face<false>(a, g, s);            \
+    return L::template vol_face<true>(a, g, s);                          \
   }
   if constexpr (sizeof(R) == 8) {
     MGC_CASE(0, false)
@@ -183,6 +226,26 @@ inline int dispatch_order(int op, int ns, bool mix, const DGArgs<R>& a, const Ga
   }
 #undef MGC_CASE
   return MGC_E_UNSUPPORTED;
+}
+
+template <class R, int DIM, int ORDER>
+inline size_t vol_workspace_order(int ns, bool mix, int64_t nelem, int64_t nbf, size_t* off_s0,
+                                  size_t* off_bt, size_t* off_bp) {
+#define MGC_WS(NSV, MIXV)                                                                  \
+  if (ns == NSV && mix == MIXV)                                                            \
+    return Launch<R, DIM, ORDER, NSV, MIXV>::vol_workspace_parts(nelem, nbf, off_s0, off_bt,   \
+                                                                 off_bp);
+  if constexpr (sizeof(R) == 8) {
+    MGC_WS(0, false)
+    MGC_WS(2, false)
+    MGC_WS(7, false)
+    MGC_WS(7, true)
+  } else {
+    MGC_WS(0, false)
+    MGC_WS(7, true)
+  }
+#undef MGC_WS
+  return 0;
 }
 
 template <class R, int DIM, int ORDER>
@@ -229,14 +292,14 @@ inline int mixture_state_mixed_dim(int ns, int64_t nnodes, const float* q, const
 
 template <class R, int DIM>
 inline int mixture_state_dim(int ns, int64_t nnodes, const R* q, const R* tseed, R* t1, R* t2,
-                             const GasParams& g, cudaStream_t s) {
+                             int32_t* status, const GasParams& g, cudaStream_t s) {
   if (ns != 7) return MGC_E_UNSUPPORTED;
   const int nt = 256;
   auto kern = k_mixture_state<R, DIM, 7>;   // grid-stride: one wave of resident blocks
   int nb = 0;
   const int rc = persistent_grid(kern, nt, 0, (nnodes + nt - 1) / nt, &nb);
   if (rc) return rc;
-  kern<<<(unsigned)nb, nt, 0, s>>>(nnodes, q, tseed, t1, t2, g);
+  kern<<<(unsigned)nb, nt, 0, s>>>(nnodes, q, tseed, t1, t2, status, g);
   return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
 }
 

@@ -54,11 +54,37 @@ struct DGArgs {
   int32_t pad_;
   R* fbuf;             // split path: per-node flux record [E*NP][FW]
   R* srcbuf;           // split path: species sources [NS][E][NP]
-  void* mid_event;     // split path (host side): cudaEvent_t recorded between
-                       // the node-flux and surface kernels, or null
+  void* mid_event;     // host side: cudaEvent_t recorded between the two
+                       // kernels of a two-kernel pass, or null
+  // volume/face path
+  R* trace;            // [E][NF][NFP][TW] face-node records: F.n, lambda, p, c, gamma
+  R* s0;               // [E][NF][NC] node-0 flux . n per face (element-constant shift)
+  R* btrace;           // [nbf][NFP][TW] exterior records of boundary faces
+  R* bplus;            // [NC][nbf][NFP] exterior q of the inviscid flux at boundary faces
+  const uint8_t* fslot;  // [nperm][NFP] neighbour face slot fn * NFP + m'
+  R* grad_out;         // optional [NC+1][DIM][E][NP] gradients (return_gradients)
 };
 
-enum BoundaryKind { BK_DUMMY = 0, BK_PRESCRIBED = 1 };
+// Boundary face kinds (int8 per boundary face).  Prescribed: exterior state
+// from the caller (boundary.py:796-1009).  The others are the Mengaldo
+// treatment (boundary.py:391-793) with their states computed on the device
+// from the interior trace; their parameters travel in the exterior-state
+// array: the wall temperature in the temperature row (isothermal), the free
+// stream state (far field), the boundary pressure in row 0 (outflow).
+enum BoundaryKind {
+  BK_DUMMY = 0,
+  BK_PRESCRIBED = 1,
+  BK_SLIP = 2,          // AdiabaticSlipBoundary          boundary.py:1052-1143
+  BK_NOSLIP = 3,        // AdiabaticNoslipWallBoundary    boundary.py:1794-1858
+  BK_ISOTHERMAL = 4,    // IsothermalWallBoundary         boundary.py:1727-1792
+  BK_FARFIELD = 5,      // FarfieldBoundary               boundary.py:1146-1228
+  BK_OUTFLOW = 6,       // PressureOutflowBoundary        boundary.py:1231-1403
+};
+__host__ __device__ constexpr bool bk_mengaldo(int k) { return k >= BK_SLIP && k <= BK_OUTFLOW; }
+// kinds whose exterior-state array entries are read
+__host__ __device__ constexpr bool bk_needs_bext(int k) {
+  return k == BK_PRESCRIBED || k == BK_ISOTHERMAL || k == BK_FARFIELD || k == BK_OUTFLOW;
+}
 
 
 __host__ __device__ constexpr int imin(int a, int b) { return a < b ? a : b; }
@@ -321,22 +347,39 @@ __device__ __forceinline__ void stage_conn(const int32_t* __restrict__ conn_g, i
 
 // {{{ mixture temperature
 
-// plain form: T1 = Newton(seed), T2 = Newton(T1), fixed iteration count
+// plain form: T1 = Newton(seed), T2 = Newton(T1), fixed iteration count.
+// The reference's fixed-count solve has no convergence check (its drivers
+// check the temperature update: mirgecom examples/autoignition.py:526-530);
+// here a node whose T2 (or, without T2, one further Newton step) moved by
+// more than 1e-6 of T1, or whose temperature is not positive and finite,
+// sets ST_NEWTON_MISS in *status*.  The temperatures written are the
+// reference's either way.
 template <class R, int DIM, int NS>
 __global__ void __launch_bounds__(256) k_mixture_state(int64_t nnodes, const R* __restrict__ q,
                                                        const R* __restrict__ tseed,
                                                        R* __restrict__ t1, R* __restrict__ t2,
-                                                       GasParams g) {
+                                                       int32_t* status, GasParams g) {
   constexpr int NC = DIM + 2 + NS;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  bool miss = false;
   for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < nnodes; n += stride) {
     R qq[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) qq[c] = q[(int64_t)c * nnodes + n];
     const R ta = node_temperature<R, DIM, NS>(qq, tseed[n], g);
     t1[n] = ta;
-    if (t2) t2[n] = node_temperature<R, DIM, NS>(qq, ta, g);
+    R tb;
+    if (t2) {
+      tb = node_temperature<R, DIM, NS>(qq, ta, g);
+      t2[n] = tb;
+    } else {
+      GasParams g1 = g;
+      g1.niter = 1;
+      tb = node_temperature<R, DIM, NS>(qq, ta, g1);
+    }
+    miss |= !(ta > R(0) && tb > R(0) && fabs(tb - ta) <= R(1e-6) * ta && ta < R(1e30));
   }
+  if (miss && status) atomicOr(status, ST_NEWTON_MISS);
 }
 
 // mixed form: float32 Newton from the learned guess (if given) else the
@@ -524,7 +567,8 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
         const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
         if (kind == BK_PRESCRIBED) {
           mode = 1;
-        } else if (kind < 0) {
+        } else if (kind != BK_DUMMY) {
+          // unknown kind, or one only the volume/face path evaluates
           atomicOr(a.status, ST_BAD_INDEX);
         }
       }
@@ -816,7 +860,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
         make_state<R, DIM, NS>(qp, MIX ? a.bext[NC * bstride + (int64_t)bf * NFP + m] : R(0),
                                g, sp);
       } else {
-        if (kind < 0) atomicOr(a.status, ST_BAD_INDEX);
+        if (kind != BK_DUMMY) atomicOr(a.status, ST_BAD_INDEX);
         mode = 1;
       }
     }
@@ -1159,7 +1203,7 @@ __device__ __noinline__ void surface_face_general(const DGArgs<R> a, const GasPa
         fpn[c] = acc;
       }
     } else {
-      if (kind < 0) atomicOr(a.status, ST_BAD_INDEX);
+      if (kind != BK_DUMMY) atomicOr(a.status, ST_BAD_INDEX);
       mode = 1;
     }
   }

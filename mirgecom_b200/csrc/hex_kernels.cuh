@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(256, 2) k_hex_grad(DGArgs<R> a, GasParams g) {
         const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
         if (kind == BK_PRESCRIBED)
           mode = 1;
-        else if (kind < 0)
+        else if (kind != BK_DUMMY)   // unknown, or a kind the hexahedra do not evaluate
           atomicOr(a.status, ST_BAD_INDEX);
       }
       R* scol = s_s + e * NU * NFN + fm;

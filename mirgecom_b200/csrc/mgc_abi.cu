@@ -15,7 +15,7 @@ int tu3_upload_mechanism(const Mechanism*);
 int tu2_dispatch(int, int, int, bool, const DGArgs<double>&, const GasParams&, cudaStream_t);
 int tu3_dispatch(int, int, int, bool, const DGArgs<double>&, const GasParams&, cudaStream_t);
 int tu2_mixture_state(int, int64_t, const double*, const double*, double*, double*,
-                      const GasParams&, cudaStream_t);
+                      int32_t*, const GasParams&, cudaStream_t);
 int tu2f_upload_refops(int, int, const double*, const float*, const int*);
 int tu3f_upload_refops(int, int, const double*, const float*, const int*);
 int tu2f_upload_mechanism(const Mechanism*);
@@ -28,11 +28,15 @@ int tu2f_mixture_state(int, int64_t, const float*, const float*, const float*, f
 int tu3f_mixture_state(int, int64_t, const float*, const float*, const float*, float*, int32_t*,
                        int, float, int32_t*, const GasParams&, cudaStream_t);
 int tu3_mixture_state(int, int64_t, const double*, const double*, double*, double*,
-                      const GasParams&, cudaStream_t);
+                      int32_t*, const GasParams&, cudaStream_t);
 size_t tu2_split_workspace(int, int, bool, int64_t);
 size_t tu3_split_workspace(int, int, bool, int64_t);
 size_t tu2f_split_workspace(int, int, bool, int64_t);
 size_t tu3f_split_workspace(int, int, bool, int64_t);
+size_t tu2_vol_workspace(int, int, bool, int64_t, int64_t, size_t*, size_t*, size_t*);
+size_t tu3_vol_workspace(int, int, bool, int64_t, int64_t, size_t*, size_t*, size_t*);
+size_t tu2f_vol_workspace(int, int, bool, int64_t, int64_t, size_t*, size_t*, size_t*);
+size_t tu3f_vol_workspace(int, int, bool, int64_t, int64_t, size_t*, size_t*, size_t*);
 int tuh_upload_hexops(const double*);
 int tuhf_upload_hexops(const double*);
 int tuh_dispatch(int, int, int, bool, const DGArgs<double>&, const GasParams&, cudaStream_t);
@@ -232,9 +236,79 @@ int rhs_split_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const
   return dispatch(visc ? 4 : 3, mesh, gas, a, (cudaStream_t)stream);
 }
 
+template <class R>
+size_t vol_ws(const mgc_mesh_t* m, const mgc_gas_t* g, size_t* off_s0, size_t* off_bt,
+              size_t* off_bp) {
+  if (m->elem_kind != kElemSimplex) return 0;
+  const bool mix = g->eos_kind == MGC_EOS_MIXTURE;
+  if constexpr (sizeof(R) == 8)
+    return m->dim == 2 ? tu2_vol_workspace(m->order, g->nspecies, mix, m->nelem, m->nbf, off_s0, off_bt, off_bp)
+                       : tu3_vol_workspace(m->order, g->nspecies, mix, m->nelem, m->nbf, off_s0, off_bt, off_bp);
+  return m->dim == 2 ? tu2f_vol_workspace(m->order, g->nspecies, mix, m->nelem, m->nbf, off_s0, off_bt, off_bp)
+                     : tu3f_vol_workspace(m->order, g->nspecies, mix, m->nelem, m->nbf, off_s0, off_bt, off_bp);
+}
+
+template <class R>
+int operator_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const R* q,
+                  const R* t_op, const R* t_src, const R* bext, int flux_kind, int add_sources,
+                  R* rhs, R* grad_out, void* workspace, size_t workspace_bytes, int32_t* status,
+                  void* stream, void* mid_event) {
+  if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !rhs || !status || !workspace)
+    return MGC_E_INVALID;
+  if (flux_kind < 0 || flux_kind > 2) return MGC_E_INVALID;
+  if (gas->eos_kind == MGC_EOS_MIXTURE && !t_op) return MGC_E_INVALID;
+  if (add_sources && (gas->eos_kind != MGC_EOS_MIXTURE || !t_src)) return MGC_E_INVALID;
+  if (grad_out && !visc) return MGC_E_INVALID;
+  if (mesh->elem_kind != kElemSimplex) return MGC_E_UNSUPPORTED;
+  if (!mesh->fslot) return MGC_E_INVALID;
+  if (reinterpret_cast<uintptr_t>(workspace) % 256) return MGC_E_INVALID;
+  int rc = ready(mesh, gas);
+  if (rc) return rc;
+  size_t off_s0 = 0, off_bt = 0, off_bp = 0;
+  const size_t need = vol_ws<R>(mesh, gas, &off_s0, &off_bt, &off_bp);
+  if (need == 0) return MGC_E_UNSUPPORTED;
+  if (workspace_bytes < need) return MGC_E_INVALID;
+  DGArgs<R> a = make_args<R>(mesh, q, t_op, t_src, nullptr, rhs, bext, flux_kind, add_sources,
+                             status);
+  char* ws = static_cast<char*>(workspace);
+  a.trace = reinterpret_cast<R*>(ws);
+  a.s0 = reinterpret_cast<R*>(ws + off_s0);
+  a.btrace = reinterpret_cast<R*>(ws + off_bt);
+  a.bplus = reinterpret_cast<R*>(ws + off_bp);
+  a.fslot = mesh->fslot;
+  a.grad_out = grad_out;
+  a.mid_event = mid_event;
+  return dispatch(visc ? 6 : 5, mesh, gas, a, (cudaStream_t)stream);
+}
+
 }  // namespace
 
 extern "C" {
+
+size_t mgc_operator_workspace_bytes(const mgc_mesh_t* mesh, const mgc_gas_t* gas,
+                                    int single_precision) {
+  if (!mesh_ok(mesh) || !gas_ok(gas)) return 0;
+  return single_precision ? vol_ws<float>(mesh, gas, nullptr, nullptr, nullptr)
+                          : vol_ws<double>(mesh, gas, nullptr, nullptr, nullptr);
+}
+
+int mgc_operator(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
+                 const double* t_op, const double* t_src, const double* bext, int flux_kind,
+                 int add_sources, double* rhs, double* grad_out, void* workspace,
+                 size_t workspace_bytes, int32_t* status, void* stream, void* mid_event) {
+  return operator_impl<double>(viscous, mesh, gas, q, t_op, t_src, bext, flux_kind, add_sources,
+                               rhs, grad_out, workspace, workspace_bytes, status, stream,
+                               mid_event);
+}
+
+int mgc_operator_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
+                     const float* t_op, const float* t_src, const float* bext, int flux_kind,
+                     int add_sources, float* rhs, float* grad_out, void* workspace,
+                     size_t workspace_bytes, int32_t* status, void* stream, void* mid_event) {
+  return operator_impl<float>(viscous, mesh, gas, q, t_op, t_src, bext, flux_kind, add_sources,
+                              rhs, grad_out, workspace, workspace_bytes, status, stream,
+                              mid_event);
+}
 
 size_t mgc_rhs_split_workspace_bytes(const mgc_mesh_t* mesh, const mgc_gas_t* gas,
                                      int single_precision) {
@@ -360,7 +434,8 @@ int mgc_set_mechanism(const mgc_mechanism_t* mech_host) {
 }
 
 int mgc_mixture_temperature(int dim, const mgc_gas_t* gas, int64_t nnodes, const double* q,
-                            const double* t_seed, double* t1, double* t2, void* stream) {
+                            const double* t_seed, double* t1, double* t2, int32_t* status,
+                            void* stream) {
   if (!gas_ok(gas) || gas->eos_kind != MGC_EOS_MIXTURE || nnodes < 0 || !q || !t_seed || !t1)
     return MGC_E_INVALID;
   if (nnodes == 0) return MGC_OK;
@@ -369,8 +444,8 @@ int mgc_mixture_temperature(int dim, const mgc_gas_t* gas, int64_t nnodes, const
   if (!g_mech_ready[dev]) return MGC_E_NOT_READY;
   const GasParams p = to_params(gas);
   cudaStream_t s = (cudaStream_t)stream;
-  if (dim == 2) return tu2_mixture_state(gas->nspecies, nnodes, q, t_seed, t1, t2, p, s);
-  if (dim == 3) return tu3_mixture_state(gas->nspecies, nnodes, q, t_seed, t1, t2, p, s);
+  if (dim == 2) return tu2_mixture_state(gas->nspecies, nnodes, q, t_seed, t1, t2, status, p, s);
+  if (dim == 3) return tu3_mixture_state(gas->nspecies, nnodes, q, t_seed, t1, t2, status, p, s);
   return MGC_E_UNSUPPORTED;
 }
 

@@ -38,4 +38,15 @@ size_t tu2f_split_workspace(int order, int ns, bool mix, int64_t nelem) {
   }
 }
 
+size_t tu2f_vol_workspace(int order, int ns, bool mix, int64_t nelem, int64_t nbf,
+                          size_t* off_s0, size_t* off_bt, size_t* off_bp) {
+  switch (order) {
+    case 1: return vol_workspace_order<float, 2, 1>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
+    case 2: return vol_workspace_order<float, 2, 2>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
+    case 3: return vol_workspace_order<float, 2, 3>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
+    case 4: return vol_workspace_order<float, 2, 4>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
+    default: return 0;
+  }
+}
+
 }  // namespace mgc

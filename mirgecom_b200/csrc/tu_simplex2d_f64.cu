@@ -21,8 +21,8 @@ int tu2_dispatch(int op, int order, int ns, bool mix, const DGArgs<double>& a,
 }
 
 int tu2_mixture_state(int ns, int64_t nnodes, const double* q, const double* tseed,
-                         double* t1, double* t2, const GasParams& g, cudaStream_t s) {
-  return mixture_state_dim<double, 2>(ns, nnodes, q, tseed, t1, t2, g, s);
+                      double* t1, double* t2, int32_t* status, const GasParams& g, cudaStream_t s) {
+  return mixture_state_dim<double, 2>(ns, nnodes, q, tseed, t1, t2, status, g, s);
 }
 
 size_t tu2_split_workspace(int order, int ns, bool mix, int64_t nelem) {
@@ -31,6 +31,17 @@ size_t tu2_split_workspace(int order, int ns, bool mix, int64_t nelem) {
     case 2: return split_workspace_order<double, 2, 2>(ns, mix, nelem);
     case 3: return split_workspace_order<double, 2, 3>(ns, mix, nelem);
     case 4: return split_workspace_order<double, 2, 4>(ns, mix, nelem);
+    default: return 0;
+  }
+}
+
+size_t tu2_vol_workspace(int order, int ns, bool mix, int64_t nelem, int64_t nbf,
+                          size_t* off_s0, size_t* off_bt, size_t* off_bp) {
+  switch (order) {
+    case 1: return vol_workspace_order<double, 2, 1>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
+    case 2: return vol_workspace_order<double, 2, 2>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
+    case 3: return vol_workspace_order<double, 2, 3>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
+    case 4: return vol_workspace_order<double, 2, 4>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
     default: return 0;
   }
 }

@@ -20,8 +20,8 @@ int tu3_dispatch(int op, int order, int ns, bool mix, const DGArgs<double>& a,
 }
 
 int tu3_mixture_state(int ns, int64_t nnodes, const double* q, const double* tseed,
-                         double* t1, double* t2, const GasParams& g, cudaStream_t s) {
-  return mixture_state_dim<double, 3>(ns, nnodes, q, tseed, t1, t2, g, s);
+                      double* t1, double* t2, int32_t* status, const GasParams& g, cudaStream_t s) {
+  return mixture_state_dim<double, 3>(ns, nnodes, q, tseed, t1, t2, status, g, s);
 }
 
 size_t tu3_split_workspace(int order, int ns, bool mix, int64_t nelem) {
@@ -29,6 +29,16 @@ size_t tu3_split_workspace(int order, int ns, bool mix, int64_t nelem) {
     case 1: return split_workspace_order<double, 3, 1>(ns, mix, nelem);
     case 2: return split_workspace_order<double, 3, 2>(ns, mix, nelem);
     case 3: return split_workspace_order<double, 3, 3>(ns, mix, nelem);
+    default: return 0;
+  }
+}
+
+size_t tu3_vol_workspace(int order, int ns, bool mix, int64_t nelem, int64_t nbf,
+                          size_t* off_s0, size_t* off_bt, size_t* off_bp) {
+  switch (order) {
+    case 1: return vol_workspace_order<double, 3, 1>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
+    case 2: return vol_workspace_order<double, 3, 2>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
+    case 3: return vol_workspace_order<double, 3, 3>(ns, mix, nelem, nbf, off_s0, off_bt, off_bp);
     default: return 0;
   }
 }

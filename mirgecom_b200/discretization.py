@@ -13,6 +13,9 @@ Device layout (all per element, elements in mesh order):
   for an interior face, ``-(1 + bface)`` for a boundary face;
 * ``perm``   uint8   [nperm, Nfp] -- volume node index, inside the neighbour,
   of the point that coincides with own face node m;
+* ``fslot``  uint8   [nperm, Nfp] -- the same point as the neighbour's face
+  slot ``fn * Nfp + m'`` (its face fn and face-node index m'), where the
+  volume kernel files the neighbour's face-node record;
 * reference operators ``W`` [d, Np, Np] and ``LIFT`` [Np, Nf*Nfp].
 
 Normals and face Jacobians are derived from ``rx`` inside the kernels
@@ -36,6 +39,7 @@ BTAG_ALL = "all"
 class FaceConnectivity:
     conn: np.ndarray           # int32 [E, Nf]
     perm: np.ndarray           # uint8 [nperm, Nfp]
+    fslot: np.ndarray          # uint8 [nperm, Nfp]
     bface_elem: np.ndarray     # int64 [nbf]
     bface_face: np.ndarray     # int64 [nbf]
     bface_side: np.ndarray     # int64 [nbf]: 2*axis + (0 low, 1 high), -1 other
@@ -102,6 +106,20 @@ def build_face_connectivity(mesh: BoxMesh, refel: ReferenceElement) -> FaceConne
     if nel * 256 >= 2 ** 31:
         raise ValueError("mesh too large for the packed face pairing")
 
+    # each permutation row lists the nodes of one neighbour face: its face
+    # slots fn * Nfp + m'
+    fslot = np.zeros(uperm.shape, dtype=np.int64)
+    fnodes = np.asarray(refel.face_nodes)
+    for pi, row in enumerate(uperm):
+        hits = [fo for fo in range(nf) if set(fnodes[fo]) == set(row)]
+        if len(hits) != 1:
+            raise RuntimeError("a face-node permutation matches no single face")
+        fo = hits[0]
+        pos = {int(k): i for i, k in enumerate(fnodes[fo])}
+        fslot[pi] = [fo * nfp + pos[int(k)] for k in row]
+    if nf * nfp > 256:
+        raise ValueError("too many face nodes for the uint8 face slots")
+
     conn = np.zeros(nel * nf, dtype=np.int64)
     conn[own] = oth_e * 256 + pinv[cinv]
     nbr_node = np.full((nel * nf, nfp), -1, dtype=np.int64)
@@ -121,6 +139,7 @@ def build_face_connectivity(mesh: BoxMesh, refel: ReferenceElement) -> FaceConne
     return FaceConnectivity(
         conn=conn.reshape(nel, nf).astype(np.int32),
         perm=uperm.astype(np.uint8),
+        fslot=fslot.astype(np.uint8),
         bface_elem=be, bface_face=bf, bface_side=side,
         nbr_node_index=nbr_node.reshape(nel, nf, nfp))
 

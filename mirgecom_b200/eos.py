@@ -160,6 +160,20 @@ class PyrometheusMixture(MixtureEOS):
         """c_p / (c_p - R_mix) (mirgecom/eos.py:644-650)."""
         return self.heat_capacity_cp(cv, temperature) / self.heat_capacity_cv(cv, temperature)
 
+    def get_density(self, pressure, temperature, species_mass_fractions):
+        """rho = p / (R_mix T) (mirgecom/eos.py:702-718)."""
+        return pressure / (self.gas_const(species_mass_fractions=species_mass_fractions)
+                           * temperature)
+
+    def get_internal_energy(self, temperature, species_mass_fractions):
+        """Mass-specific internal energy e(T, Y) = sum_k Y_k (R/W_k) T
+        (h_k/RT - 1) (mirgecom/eos.py:690-700)."""
+        from mirgecom_b200.initializers import _nasa_e_rt
+        y = species_mass_fractions
+        t = temperature
+        w = _wcol(self._mech.molecular_weights, y)
+        return GAS_CONSTANT * t * (y / w * _nasa_e_rt(self._mech, t)).sum(dim=0)
+
     def pressure(self, cv, temperature):
         """p = rho R_mix T (mirgecom/eos.py:751-761)."""
         return cv.mass * self.gas_const(cv) * temperature

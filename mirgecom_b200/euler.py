@@ -2,8 +2,11 @@
 
 ``euler_operator`` keeps the reference signature.  The RHS
 ``-div_operator(F_I, F*_I)`` -- volume flux, trace pairs, numerical flux,
-boundary fluxes, weak divergence, face lift and inverse mass -- is ONE
-device kernel launch (``mgc_euler_rhs``).
+boundary fluxes, weak divergence, face lift and inverse mass -- runs on the
+device (``runtime.euler_rhs``): on simplicial meshes two kernels through
+``mgc_operator`` (a volume kernel for the pointwise fluxes, face-node records
+and the volume part of the divergence, a face kernel for the numerical
+fluxes and the lift); on hexahedra the split divergence pass.
 """
 
 from __future__ import annotations

@@ -1,12 +1,14 @@
 """Navier-Stokes operator, mirroring mirgecom/navierstokes.py:129-575.
 
 ``ns_operator`` keeps the reference signature and computes
-div(F_V - F_I) with BR1 gradients in two device kernels: the gradient pass
-(grad_cv_operator + grad_t_operator fused, ``mgc_ns_grad``) and the
-divergence pass (``mgc_ns_rhs``).  For a reacting mixture the species source
-terms (the driver-side ``eos.get_species_source_terms`` of
-examples/gas-in-box.py:702-705) can be fused into the divergence pass by
-passing ``species_source_temperature``.
+div(F_V - F_I) with BR1 gradients on the device (``runtime.ns_rhs``): on
+simplicial meshes in two kernels through ``mgc_operator`` (a volume kernel
+that keeps the gradients on chip and evaluates the pointwise fluxes and the
+volume part of the divergence, and a face kernel for the numerical fluxes and
+the lift); on hexahedra as a gradient pass and a split divergence pass.
+For a reacting mixture the species source terms (the driver-side
+``eos.get_species_source_terms`` of examples/gas-in-box.py:702-705) are
+fused into the volume kernel by passing ``species_source_temperature``.
 """
 
 from __future__ import annotations
@@ -79,9 +81,10 @@ def ns_operator(dcoll, gas_model, state, boundaries, *, time=0.0,
         raise NotImplementedError("limiters / precomputed operator states are not supported")
     kind = flux_kind_of(inviscid_numerical_flux_func)
     rhs, grad = runtime.ns_rhs(dcoll, state, gas_model, boundaries or {}, time, kind,
-                               source_temperature=species_source_temperature)
+                               source_temperature=species_source_temperature,
+                               want_gradients=return_gradients)
     out = ConservedVars(rhs, state.dim)
     if return_gradients:
-        gcv, gt = _split_grad(grad.clone(), state)
+        gcv, gt = _split_grad(grad, state)
         return out, gcv, gt
     return out

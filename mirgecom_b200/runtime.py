@@ -17,10 +17,24 @@ from mirgecom_b200 import _lib
 
 _uploaded_refops = set()     # (device index, element kind, dim, order)
 _uploaded_mech = {}          # device index -> id(mechanism)
+_state_status = {}           # device index -> int32 status word of the state kernels
 
 
 def _dev_index(device):
     return device.index if device.index is not None else torch.cuda.current_device()
+
+
+def state_status_word(device):
+    """The int32 device word into which the temperature kernels of this
+    device OR their status bits (a fluid state is made without a
+    discretization, so its solve reports here; :func:`read_status` reads it
+    together with the discretization's word)."""
+    idx = _dev_index(device)
+    w = _state_status.get(idx)
+    if w is None:
+        w = torch.zeros(1, dtype=torch.int32, device=torch.device("cuda", idx))
+        _state_status[idx] = w
+    return w
 
 
 def ensure_reference_operators(dcoll, device):
@@ -72,6 +86,7 @@ class DeviceDiscretization:
         self.rx32 = self.rx.to(torch.float32)
         self.conn = torch.from_numpy(np.ascontiguousarray(c.conn, dtype=np.int32)).to(device)
         self.perm = torch.from_numpy(np.ascontiguousarray(c.perm, dtype=np.uint8)).to(device)
+        self.fslot = torch.from_numpy(np.ascontiguousarray(c.fslot, dtype=np.uint8)).to(device)
         nbf = len(c.bface_elem)
         self.nbf = nbf
         self.bface_elem = torch.from_numpy(c.bface_elem).to(device)
@@ -91,6 +106,7 @@ class DeviceDiscretization:
         self.mesh.perm = self.perm.data_ptr()
         self.mesh.bkind = None
         self.mesh.rx32 = self.rx32.data_ptr()
+        self.mesh.fslot = self.fslot.data_ptr()
         self.mesh.elem_kind = 1 if dcoll.refel.kind == "hypercube" else 0
 
     def workspace(self, name, shape, dtype=torch.float64):
@@ -154,7 +170,7 @@ def mixture_temperature_mixed(cv, gas_model, tseed, tguess=None, iters=None, sta
     if tguess is not None:
         tguess = tguess.to(dtype=torch.float32).contiguous()
     if status is None:
-        status = torch.zeros(1, dtype=torch.int32, device=q.device)
+        status = state_status_word(q.device)
     with torch.cuda.device(q.device):
         if learned is not None:
             ms = learned.struct()
@@ -170,8 +186,9 @@ def mixture_temperature_mixed(cv, gas_model, tseed, tguess=None, iters=None, sta
     return tout
 
 
-def mixture_temperature(cv, gas_model, tseed):
-    """Launch the Newton temperature kernel: returns (T1, T2)."""
+def mixture_temperature(cv, gas_model, tseed, status=None):
+    """Launch the Newton temperature kernel: returns (T1, T2).  Unconverged
+    nodes set ST_NEWTON_MISS in *status* (default: the device's state word)."""
     q = cv.q
     _lib.require_cuda(q)
     lib = _lib.load()
@@ -180,17 +197,27 @@ def mixture_temperature(cv, gas_model, tseed):
     t1 = torch.empty_like(q[0])
     t2 = torch.empty_like(q[0])
     tseed = tseed.to(dtype=q.dtype).contiguous()
+    if status is None:
+        status = state_status_word(q.device)
     with torch.cuda.device(q.device):
         _lib.check(lib.mgc_mixture_temperature(
             cv.dim, C.byref(gs), n, _lib.ptr(q), _lib.ptr(tseed), _lib.ptr(t1),
-            _lib.ptr(t2), _lib.stream_handle()), "mgc_mixture_temperature")
+            _lib.ptr(t2), _lib.ptr(status), _lib.stream_handle()), "mgc_mixture_temperature")
     return t1, t2
 
 
 def boundary_exterior(dd, state, gas_model, boundaries, time):
-    """[Nc+1, nbf, Nfp] exterior states of the prescribed boundaries, or None."""
-    from mirgecom_b200.boundary import PrescribedFluidBoundary
-    if not any(isinstance(b, PrescribedFluidBoundary) for b in boundaries.values()):
+    """[Nc+1, nbf, Nfp] exterior-state array of the boundary faces: the
+    exterior states of the prescribed boundaries, the parameters of the
+    Mengaldo ones (wall temperature, free stream, boundary pressure); None
+    when no boundary needs one."""
+    from mirgecom_b200.boundary import MengaldoBoundaryCondition, PrescribedFluidBoundary
+
+    def wants(b):
+        return (isinstance(b, PrescribedFluidBoundary) and b.device_kind == 1) or (
+            isinstance(b, MengaldoBoundaryCondition) and type(b).exterior_parameters
+            is not MengaldoBoundaryCondition.exterior_parameters)
+    if not any(wants(b) for b in boundaries.values()):
         return None
     dcoll = dd.dcoll
     q = state.cv.q
@@ -205,11 +232,14 @@ def boundary_exterior(dd, state, gas_model, boundaries, time):
     if state.is_mixture:
         tm = state.temperature[be, dd.bface_nodes]
     for tag, bdry in boundaries.items():
-        if not isinstance(bdry, PrescribedFluidBoundary):
+        if not wants(bdry):
             continue
         mask = torch.from_numpy(dcoll.boundary_face_mask(tag)).to(q.device)
         sm = FluidState(ConservedVars(qm[:, mask], state.dim), gas_model,
                         temperature=None if tm is None else tm[mask])
+        if isinstance(bdry, MengaldoBoundaryCondition):
+            bext[:, mask] = bdry.exterior_parameters(dcoll, gas_model, sm, nc).to(q.dtype)
+            continue
         nrm = torch.from_numpy(np.ascontiguousarray(
             dcoll.boundary_normals_numpy()[dcoll.boundary_face_mask(tag)].T)).to(q.device)
         ext = bdry.exterior_state(dcoll, tag, gas_model, sm, time,
@@ -234,9 +264,20 @@ def _operator_temperature(state):
     return state.operator_temperature.contiguous()
 
 
-# The divergence pass runs split (pointwise flux records + surface/lift
-# kernel) by default; the fused single-kernel form stays available.
-SPLIT_RHS = True
+# Which device path evaluates the right-hand side of simplicial meshes:
+#   "volume_face"  two kernels: volume (gradients kept on chip, pointwise
+#                  fluxes, face-node records, volume divergence) and face
+#                  (numerical fluxes from the records, lift) -- mgc_operator*
+#   "split"        three kernels: gradients, per-node flux records, surface
+#                  and lift -- mgc_ns_grad* + mgc_rhs_split*
+#   "fused"        two kernels: gradients, fused divergence -- mgc_ns_grad* +
+#                  mgc_ns_rhs* (mgc_euler_rhs* for the Euler operator)
+# Tensor-product hexahedra always take "split".
+RHS_PATH = "volume_face"
+
+
+def _path(dcoll):
+    return "split" if dcoll.refel.kind == "hypercube" else RHS_PATH
 
 
 def _split_workspace(dd, gs, f32):
@@ -247,6 +288,39 @@ def _split_workspace(dd, gs, f32):
     return dd.workspace("split_ws", ((nbytes + 15) // 16 * 16,), torch.uint8)
 
 
+def _operator_workspace(dd, gs, f32):
+    lib = _lib.load()
+    nbytes = lib.mgc_operator_workspace_bytes(C.byref(dd.mesh), C.byref(gs), int(f32))
+    if nbytes == 0:
+        raise RuntimeError("volume/face right-hand side unsupported for this configuration")
+    # torch allocations are 256-byte aligned, as the entry point requires
+    return dd.workspace("operator_ws", ((nbytes + 255) // 256 * 256,), torch.uint8)
+
+
+def _run_operator(viscous, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs, grad_out,
+                  events=None):
+    """mgc_operator*: volume kernel then face kernel.  *events* (3 CUDA
+    events): recorded before the volume kernel, between the two kernels and
+    after the face kernel."""
+    lib = _lib.load()
+    f32 = q.dtype == torch.float32
+    ws = _operator_workspace(dd, gs, f32)
+    fn = lib.mgc_operator_f32 if f32 else lib.mgc_operator
+    mid = None
+    if events:
+        events[0].record()
+        # the event exists once recorded; the library records it again
+        # between its two kernels
+        events[1].record()
+        mid = events[1].cuda_event
+    _lib.check(fn(int(viscous), C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op),
+                  _lib.ptr(t_src), _lib.ptr(bext), flux_kind, int(add_src), _lib.ptr(rhs),
+                  _lib.ptr(grad_out), _lib.ptr(ws), ws.numel(), _lib.ptr(dd.status),
+                  _lib.stream_handle(), mid), "mgc_operator")
+    if events:
+        events[2].record()
+
+
 def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
     q = state.cv.q
     _lib.require_cuda(q)
@@ -254,46 +328,58 @@ def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
     lib = _lib.load()
     dd = device_discretization(dcoll, q.device)
     gs = _gas_struct(gas_model, state.cv.nspecies, q.device)
+    if _path(dcoll) != "volume_face":
+        # the inviscid slip wall needs only its state_plus: prescribe it
+        from mirgecom_b200.boundary import AdiabaticSlipBoundary, _SlipStatePlus
+        boundaries = {t: (_SlipStatePlus() if isinstance(b, AdiabaticSlipBoundary) else b)
+                      for t, b in boundaries.items()}
+    _check_boundary_path(dcoll, boundaries)
     bkind = dd.bkind_for(boundaries)
     dd.mesh.bkind = bkind.data_ptr()
     bext = boundary_exterior(dd, state, gas_model, boundaries, time)
     t_op = _operator_temperature(state)
     rhs = torch.empty_like(q)
     f32 = q.dtype == torch.float32
-    if SPLIT_RHS:
-        ws = _split_workspace(dd, gs, f32)
-        fsplit = lib.mgc_rhs_split_f32 if f32 else lib.mgc_rhs_split
-        with torch.cuda.device(q.device):
+    path = _path(dcoll)
+    with torch.cuda.device(q.device):
+        if path == "volume_face":
+            _run_operator(False, dd, gs, q, t_op, None, bext, flux_kind, False, rhs, None)
+        elif path == "split":
+            ws = _split_workspace(dd, gs, f32)
+            fsplit = lib.mgc_rhs_split_f32 if f32 else lib.mgc_rhs_split
             _lib.check(fsplit(0, C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op),
                               None, None, _lib.ptr(bext), flux_kind, 0, _lib.ptr(rhs),
                               _lib.ptr(ws), ws.numel(), _lib.ptr(dd.status),
                               _lib.stream_handle(), None), "mgc_rhs_split")
-        return rhs
-    fn = lib.mgc_euler_rhs_f32 if f32 else lib.mgc_euler_rhs
-    with torch.cuda.device(q.device):
-        _lib.check(fn(
-            C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(bext),
-            flux_kind, _lib.ptr(rhs), _lib.ptr(dd.status), _lib.stream_handle()),
-            "mgc_euler_rhs")
+        else:
+            fn = lib.mgc_euler_rhs_f32 if f32 else lib.mgc_euler_rhs
+            _lib.check(fn(
+                C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(bext),
+                flux_kind, _lib.ptr(rhs), _lib.ptr(dd.status), _lib.stream_handle()),
+                "mgc_euler_rhs")
     return rhs
 
 
-def _refuse_inviscid_only(boundaries):
-    """The viscous treatment of a wall that only the inviscid operator
-    supports (the slip wall) is not built."""
-    bad = [t for t, b in boundaries.items() if getattr(b, "inviscid_only", False)]
-    if bad:
+def _check_boundary_path(dcoll, boundaries):
+    """The Mengaldo boundaries are evaluated by the volume/face path only."""
+    from mirgecom_b200.boundary import MengaldoBoundaryCondition
+    bad = [t for t, b in boundaries.items() if isinstance(b, MengaldoBoundaryCondition)]
+    if bad and _path(dcoll) != "volume_face":
         raise NotImplementedError(
-            f"boundaries {bad}: only their inviscid treatment is built (euler_operator)")
+            f"boundaries {bad}: the Mengaldo treatment runs on the volume/face path of "
+            "simplicial meshes only")
 
 
 def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
-           source_temperature=None, grad_out=None, events=None):
-    """Gradient + divergence passes.  *events* (3 or 4 CUDA events) are
-    recorded before the gradient pass, between the passes, (with 4: between
-    the node-flux and surface kernels of the split divergence) and after the
-    divergence."""
-    _refuse_inviscid_only(boundaries)
+           source_temperature=None, want_gradients=False, events=None):
+    """The Navier-Stokes right-hand side; returns (rhs, gradients or None).
+    Gradients [Nc+1, dim, E, Np] are returned when *want_gradients* (they are
+    only written to HBM then, on the volume/face path).  *events*: on the
+    volume/face path 3 CUDA events (before the volume kernel, between the
+    two kernels, after the face kernel); on the other paths 3 or 4 (before
+    the gradient pass, between the passes, [between the node-flux and surface
+    kernels,] after the divergence)."""
+    _check_boundary_path(dcoll, boundaries)
     q = state.cv.q
     _lib.require_cuda(q)
     q = q.contiguous()
@@ -305,8 +391,6 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
     dd.mesh.bkind = bkind.data_ptr()
     bext = boundary_exterior(dd, state, gas_model, boundaries, time)
     t_op = _operator_temperature(state)
-    grad = grad_out if grad_out is not None else dd.workspace(
-        "grad", (nc + 1, dcoll.dim) + tuple(q.shape[1:]), q.dtype)
     if source_temperature is not None:
         source_temperature = source_temperature.to(q.dtype)
     rhs = torch.empty_like(q)
@@ -314,6 +398,15 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
     add_src = source_temperature is not None
     t_src = source_temperature.contiguous() if add_src else None
     f32 = q.dtype == torch.float32
+    path = _path(dcoll)
+    gshape = (nc + 1, dcoll.dim) + tuple(q.shape[1:])
+    if path == "volume_face":
+        grad = torch.empty(gshape, dtype=q.dtype, device=q.device) if want_gradients else None
+        with torch.cuda.device(q.device):
+            _run_operator(True, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs, grad,
+                          events=events)
+        return rhs, grad
+    grad = dd.workspace("grad", gshape, q.dtype)
     fgrad = lib.mgc_ns_grad_f32 if f32 else lib.mgc_ns_grad
     frhs = lib.mgc_ns_rhs_f32 if f32 else lib.mgc_ns_rhs
     with torch.cuda.device(q.device):
@@ -324,13 +417,11 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
             _lib.ptr(grad), _lib.ptr(dd.status), stream), "mgc_ns_grad")
         if events:
             events[1].record()
-        if SPLIT_RHS:
+        if path == "split":
             ws = _split_workspace(dd, gs, f32)
             fsplit = lib.mgc_rhs_split_f32 if f32 else lib.mgc_rhs_split
             mid = None
             if events and len(events) == 4:
-                # the event exists once recorded; the library records it
-                # again between its two kernels
                 events[2].record()
                 mid = events[2].cuda_event
             _lib.check(fsplit(1, C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op),
@@ -344,16 +435,19 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
                 _lib.ptr(dd.status), stream), "mgc_ns_rhs")
         if events:
             events[-1].record()
-    return rhs, grad
+    return rhs, (grad.clone() if want_gradients else None)
 
 
 def read_status(dcoll, device=None, reset=True):
-    """Device status bits accumulated by the kernels (synchronises)."""
+    """Device status bits accumulated by the kernels of *dcoll* and by the
+    device's temperature kernels (synchronises)."""
     device = device or torch.device("cuda", torch.cuda.current_device())
     dd = device_discretization(dcoll, device)
-    val = int(dd.status.item())
+    sw = state_status_word(device)
+    val = int(dd.status.item()) | int(sw.item())
     if reset:
         dd.status.zero_()
+        sw.zero_()
     return val
 
 
@@ -371,8 +465,14 @@ def rk4_stage(q0, k, acc, qout, stage, dt, qout_lo=None):
 
 
 def ns_gradients(dcoll, state, gas_model, boundaries, time):
-    """Gradient pass only: [Nc+1, dim, E, Np] (workspace tensor)."""
-    _refuse_inviscid_only(boundaries)
+    """The BR1 gradients [Nc+1, dim, E, Np] (a workspace tensor): the gradient
+    kernel mgc_ns_grad*, or, where a Mengaldo boundary needs the volume/face
+    path's boundary treatment, that path's gradient output."""
+    from mirgecom_b200.boundary import MengaldoBoundaryCondition
+    if any(isinstance(b, MengaldoBoundaryCondition) for b in boundaries.values()):
+        _check_boundary_path(dcoll, boundaries)
+        _, grad = ns_rhs(dcoll, state, gas_model, boundaries, time, 0, want_gradients=True)
+        return grad
     q = state.cv.q
     _lib.require_cuda(q)
     q = q.contiguous()

@@ -14,7 +14,10 @@ Restates the reference's operator sequence one numpy operation at a time:
   (``project_fluid_state``, ``make_fluid_state_trace_pairs``,
   ``make_operator_fluid_states``), including the mixture temperature solve on
   both sides of every face seeded by the restricted volume temperature;
-* boundaries: mirgecom/boundary.py:796-1049 (Prescribed and Dummy).
+* boundaries: mirgecom/boundary.py:796-1049 (Prescribed and Dummy) and the
+  Mengaldo treatment of boundary.py:391-793 with its walls and flow
+  boundaries (AdiabaticSlip :1052, Farfield :1146, PressureOutflow :1231,
+  IsothermalWall :1727, AdiabaticNoslipWall :1794).
 
 The connectivity is built here independently of the product (face matching
 by centroid k-d tree, node matching by coordinates), and compared with the
@@ -213,11 +216,230 @@ class PrescribedBoundary:
         self.func = func
 
 
-class AdiabaticSlipBoundary:
-    """mirgecom/boundary.py:1052-1080 (state_plus) with the slip component's
-    momentum_plus (boundary.py:152-153): for the inviscid flux the exterior
-    state is the interior one with its normal momentum reflected, m+ = m -
-    2 (m . n) n.  The viscous (Mengaldo) wall treatment is not restated."""
+# {{{ Mengaldo boundaries
+
+def _internal_energy(gas, t, y):
+    """eos.get_internal_energy: mass-specific internal energy at T (and Y)
+    (mirgecom/eos.py:459-470 ideal, :690-700 mixture)."""
+    if isinstance(gas, ph.IdealGas):
+        return gas.gas_const / (gas.gamma - 1.0) * t
+    return ph.mixture_e_mass(gas.mech, t, y)
+
+
+def _gas_const(gas, y):
+    if isinstance(gas, ph.IdealGas):
+        return gas.gas_const
+    return ph.mixture_gas_const(gas.mech, y)
+
+
+def _replace_state(sm, gas, transport, dim, energy=None, momentum=None):
+    """mirgecom/gas_model.py:907-997 (replace_fluid_state): the interior
+    state's conserved variables with *energy* / *momentum* replaced, its
+    temperature re-solved from the interior temperature."""
+    q = sm["cv"].copy()
+    if energy is not None:
+        q[1] = energy
+    if momentum is not None:
+        q[2:2 + dim] = momentum
+    seed = sm["temperature"] if isinstance(gas, ph.MixtureGas) else None
+    return ph.make_fluid_state(q, gas, transport, dim, temperature_seed=seed)
+
+
+def _dot(a, b):
+    return np.sum(a * b, axis=0)
+
+
+def _grad_species_impermeable(sm, gcv, nb, dim):
+    """mirgecom/boundary.py:187-204: the species mass fractions' normal
+    gradient removed, grad(rho Y)_bc = rho grad(Y)_bc + Y grad(rho)."""
+    q = sm["cv"]
+    rho = q[0]
+    ns = q.shape[0] - 2 - dim
+    out = gcv[2 + dim:].copy()
+    for k in range(ns):
+        y = q[2 + dim + k] / rho
+        gy = (gcv[2 + dim + k] - y * gcv[0]) / rho          # fluid.py:400-427
+        gy_bc = gy - _dot(gy, nb) * nb
+        out[k] = rho * gy_bc + y * gcv[0]
+    return out
+
+
+def _grad_velocity_slip(sm, gcv, nb, dim):
+    """mirgecom/boundary.py:156-172: the velocity gradient rotated into the
+    boundary frame (normal, tangents), the tangential velocities' normal
+    derivatives zeroed, rotated back.  Written as the equivalent projection
+    G - (I - n n^T) G n n^T, G[i][j] = d v_i / d x_j: the reference's
+    frame (boundary.py:75-117) divides by the normal's z component, which
+    vanishes on x and y walls in 3-D; the projection is the same tensor
+    wherever that frame is defined (tests/test_mengaldo_oracle.py)."""
+    q = sm["cv"]
+    rho = q[0]
+    v = q[2:2 + dim] / rho
+    g = (gcv[2:2 + dim] - v[:, None] * gcv[0][None]) / rho    # fluid.py:355-397
+    gn = np.einsum("ij...,j...->i...", g, nb)                 # G n
+    tang = gn - _dot(gn, nb) * nb                             # (I - n n^T) G n
+    return g - tang[:, None] * nb[None, :]
+
+
+class MengaldoBoundary:
+    """mirgecom/boundary.py:391-793.  Inviscid flux: the numerical flux
+    between the interior state and :meth:`state_plus`; gradient fluxes:
+    state_bc.cv (x) n and temperature_bc n (:732-793); viscous flux:
+    F_V(state_bc, grad_cv_bc, grad_t_bc) . n (:654-730, not the central
+    flux).  States are functions of the interior boundary state *sm*, the
+    normals *nb* (dim, nbf, 1) and the gas."""
+
+    def state_plus(self, sm, gas, tr, nb, dim):
+        raise NotImplementedError
+
+    def state_bc(self, sm, gas, tr, nb, dim):
+        raise NotImplementedError
+
+    def temperature_bc(self, sm):
+        return sm["temperature"]
+
+    def grad_cv_bc(self, sm, sbc, gcv, nb, dim):
+        return gcv
+
+    def grad_t_bc(self, gt, nb):
+        return gt
+
+
+class AdiabaticSlipBoundary(MengaldoBoundary):
+    """mirgecom/boundary.py:1052-1143 with the slip, impermeable and
+    adiabatic components (:149-204)."""
+
+    def state_plus(self, sm, gas, tr, nb, dim):
+        m = sm["cv"][2:2 + dim]
+        return _replace_state(sm, gas, tr, dim, momentum=m - 2.0 * _dot(m, nb) * nb)
+
+    def state_bc(self, sm, gas, tr, nb, dim):
+        q = sm["cv"]
+        m = q[2:2 + dim]
+        m_bc = m - _dot(m, nb) * nb
+        rho_e = q[1] - 0.5 * _dot(m, m) / q[0]                 # eos.internal_energy
+        return _replace_state(sm, gas, tr, dim, energy=rho_e + 0.5 * _dot(m_bc, m_bc) / q[0],
+                              momentum=m_bc)
+
+    def grad_cv_bc(self, sm, sbc, gcv, nb, dim):
+        gv_bc = _grad_velocity_slip(sm, gcv, nb, dim)
+        v_bc = sbc["cv"][2:2 + dim] / sbc["cv"][0]
+        out = gcv.copy()
+        out[2:2 + dim] = sbc["cv"][0] * gv_bc + v_bc[:, None] * gcv[0][None]
+        out[2 + dim:] = _grad_species_impermeable(sm, gcv, nb, dim)
+        return out
+
+    def grad_t_bc(self, gt, nb):
+        return gt - _dot(gt, nb) * nb
+
+
+class AdiabaticNoslipWallBoundary(MengaldoBoundary):
+    """mirgecom/boundary.py:1794-1858."""
+
+    def state_plus(self, sm, gas, tr, nb, dim):
+        return _replace_state(sm, gas, tr, dim, momentum=-sm["cv"][2:2 + dim])
+
+    def _t_wall(self, sm):
+        return sm["temperature"]
+
+    def state_bc(self, sm, gas, tr, nb, dim):
+        q = sm["cv"]
+        y = q[2 + dim:] / q[0]
+        e_bc = q[0] * _internal_energy(gas, self._t_wall(sm), y)
+        return _replace_state(sm, gas, tr, dim, energy=e_bc, momentum=0.0 * q[2:2 + dim])
+
+    def temperature_bc(self, sm):
+        return self._t_wall(sm)
+
+    def grad_cv_bc(self, sm, sbc, gcv, nb, dim):
+        out = gcv.copy()
+        out[2 + dim:] = _grad_species_impermeable(sm, gcv, nb, dim)
+        return out
+
+    def grad_t_bc(self, gt, nb):
+        return gt - _dot(gt, nb) * nb
+
+
+class IsothermalWallBoundary(AdiabaticNoslipWallBoundary):
+    """mirgecom/boundary.py:1727-1792."""
+
+    def __init__(self, wall_temperature=300.0):
+        self.wall_temperature = wall_temperature
+
+    def _t_wall(self, sm):
+        return np.zeros_like(sm["temperature"]) + self.wall_temperature
+
+    def grad_t_bc(self, gt, nb):
+        return gt
+
+
+class FarfieldBoundary(MengaldoBoundary):
+    """mirgecom/boundary.py:1146-1228: both states are the free stream."""
+
+    def __init__(self, free_stream_pressure, free_stream_velocity, free_stream_temperature,
+                 free_stream_mass_fractions=None):
+        self.p = free_stream_pressure
+        self.v = np.asarray(free_stream_velocity, dtype=np.float64)
+        self.t = free_stream_temperature
+        self.y = (None if free_stream_mass_fractions is None
+                  else np.asarray(free_stream_mass_fractions, dtype=np.float64))
+
+    def state_plus(self, sm, gas, tr, nb, dim):
+        shape = sm["cv"][0].shape
+        ns = sm["cv"].shape[0] - 2 - dim
+        t = np.zeros(shape) + self.t
+        y = (np.zeros((ns,) + shape) + self.y.reshape((-1,) + (1,) * len(shape))
+             if ns else np.zeros((0,) + shape))
+        rho = self.p / (_gas_const(gas, y) * t)
+        v = np.zeros((dim,) + shape) + self.v.reshape((-1,) + (1,) * len(shape))
+        e = _internal_energy(gas, t, y)
+        q = np.concatenate([rho[None], (rho * (e + 0.5 * _dot(v, v)))[None], rho * v, rho * y])
+        seed = t if isinstance(gas, ph.MixtureGas) else None
+        return ph.make_fluid_state(q, gas, tr, dim, temperature_seed=seed)
+
+    def state_bc(self, sm, gas, tr, nb, dim):
+        return self.state_plus(sm, gas, tr, nb, dim)
+
+    def temperature_bc(self, sm):
+        return np.zeros_like(sm["temperature"]) + self.t
+
+
+class PressureOutflowBoundary(MengaldoBoundary):
+    """mirgecom/boundary.py:1231-1403: mass, momentum and species from the
+    interior; the energy from the prescribed pressure where the outflow is
+    subsonic (|v . n| <= c), from the interior where it is supersonic."""
+
+    def __init__(self, boundary_pressure=101325.0):
+        self.p = boundary_pressure
+
+    def _state(self, sm, gas, tr, nb, dim, pressure_plus):
+        q = sm["cv"]
+        rho = q[0]
+        m = q[2:2 + dim]
+        v = m / rho
+        vn = _dot(v, nb)
+        speed = np.sqrt(_dot(vn * nb, vn * nb))
+        ke = 0.5 * _dot(m, m) / rho
+        supersonic = speed > sm["speed_of_sound"]
+        if isinstance(gas, ph.MixtureGas):
+            y = q[2 + dim:] / rho
+            t_plus = np.where(supersonic, sm["temperature"],
+                              pressure_plus / (rho * _gas_const(gas, y)))
+            rho_e = rho * _internal_energy(gas, t_plus, y)
+        else:
+            pb = np.where(supersonic, sm["pressure"], pressure_plus)
+            rho_e = pb / (sm["gamma"] - 1.0)
+        return _replace_state(sm, gas, tr, dim, energy=rho_e + ke)
+
+    def state_plus(self, sm, gas, tr, nb, dim):
+        p_plus = np.where(sm["pressure"] > 2.0 * self.p, sm["pressure"],
+                          2.0 * self.p - sm["pressure"])
+        return self._state(sm, gas, tr, nb, dim, p_plus)
+
+    def state_bc(self, sm, gas, tr, nb, dim):
+        return self._state(sm, gas, tr, nb, dim, self.p + 0.0 * sm["pressure"])
+
+# }}}
 
 
 def _normalize_boundaries(boundaries):
@@ -265,12 +487,11 @@ def make_operator_fluid_states(disc, state, gas, transport, boundaries, time):
         sm = ph.make_fluid_state(qb, gas, transport, dim, temperature_seed=tb)
         if isinstance(bdry, DummyBoundary):
             sp = sm
-        elif isinstance(bdry, AdiabaticSlipBoundary):
+        elif isinstance(bdry, MengaldoBoundary):
             nb = _bnormals(disc)
-            qe = qb.copy()
-            mom = qe[2:2 + dim]
-            qe[2:2 + dim] = mom - 2.0 * np.sum(mom * nb, axis=0) * nb
-            sp = ph.make_fluid_state(qe, gas, transport, dim, temperature_seed=tb)
+            sp = bdry.state_plus(sm, gas, transport, nb, dim)
+            sp["bc"] = bdry.state_bc(sm, gas, transport, nb, dim)
+            sp["temperature_bc"] = bdry.temperature_bc(sm)
         else:
             xb = disc.nodes[:, be[:, None], fnodes]
             ext = bdry.func(xb, time)
@@ -339,6 +560,8 @@ def grad_cv_operator(disc, ostates, time=0.0):
     for tag, (bdry, sm, sp, mask) in bst.items():
         if isinstance(bdry, DummyBoundary):
             fb = np.array([sm["cv"] * bn[j] for j in range(disc.dim)])   # :1031
+        elif isinstance(bdry, MengaldoBoundary):
+            fb = np.array([sp["bc"]["cv"] * bn[j] for j in range(disc.dim)])  # :732-760
         else:
             fb = np.array([sp["cv"] * bn[j] for j in range(disc.dim)])   # :895-907
         flux = flux + _scatter_boundary(disc, fb, flux.shape, mask)
@@ -353,8 +576,13 @@ def grad_t_operator(disc, ostates, time=0.0):
     flux = flux * disc.interior_mask[None, :, :, None]
     bn = _bnormals(disc)
     for tag, (bdry, sm, sp, mask) in bst.items():
-        src = sm if isinstance(bdry, DummyBoundary) else sp
-        fb = np.array([src["temperature"] * bn[j] for j in range(disc.dim)])
+        if isinstance(bdry, DummyBoundary):
+            tb = sm["temperature"]
+        elif isinstance(bdry, MengaldoBoundary):
+            tb = sp["temperature_bc"]                                     # :762-793
+        else:
+            tb = sp["temperature"]
+        fb = np.array([tb * bn[j] for j in range(disc.dim)])
         flux = flux + _scatter_boundary(disc, fb, flux.shape, mask)
     return grad_operator(disc, vol["temperature"], flux)
 
@@ -377,6 +605,12 @@ def viscous_flux_on_element_boundary(disc, ostates, grad_cv, grad_t):
     for tag, (bdry, sm, sp, mask) in bst.items():
         if isinstance(bdry, DummyBoundary):
             fb = ph.dot_normal(ph.viscous_flux(sm, gcv_b, gt_b), bn)     # :1047
+        elif isinstance(bdry, MengaldoBoundary):
+            # F_V(state_bc, grad_cv_bc, grad_t_bc) . n (boundary.py:654-730)
+            sbc = sp["bc"]
+            gcv_bc = bdry.grad_cv_bc(sm, sbc, gcv_b, bn, disc.dim)
+            gt_bc = bdry.grad_t_bc(gt_b, bn)
+            fb = ph.dot_normal(ph.viscous_flux(sbc, gcv_bc, gt_bc), bn)
         else:
             # central flux, exterior gradients = interior (boundary.py:141-146)
             fb = ph.viscous_facial_flux_central(sm, sp, gcv_b, gcv_b, gt_b, gt_b, bn)

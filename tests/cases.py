@@ -19,22 +19,40 @@ def rel_l2(a, b):
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
 
 
-def field_rel_l2(a, b, floor=None):
-    """Largest per-field relative L2 error (fields along axis 0).
+def field_errors(a, b, floor=None):
+    """Per-field relative L2 errors (fields along axis 0), two ways.
 
-    A field whose reference is zero up to roundoff (e.g. grad(rho) for a
-    uniform density) is measured against ``floor[c]`` (its natural scale)
-    or, by default, 1e-3 of the largest field norm, instead of its own
-    norm."""
+    Returns (own, floored): *own* divides by each field's own norm; *floored*
+    divides by the larger of that norm and ``floor[c]``, the field's natural
+    physical scale (|q_c|/h for a gradient, |F_c|/h for a divergence: see
+    :func:`flux_scale_floor`), for fields whose value is a small difference of
+    large fluxes (low-Mach momentum, a uniform density's gradient).  Without
+    *floor* the two are equal."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
-    big = max(np.linalg.norm(b[c].ravel()) for c in range(b.shape[0]))
-    errs = []
+    own, fl = [], []
     for c in range(b.shape[0]):
-        fl = 1e-3 * big if floor is None else floor[c]
-        den = max(np.linalg.norm(b[c].ravel()), fl, 1e-300)
-        errs.append(np.linalg.norm((a[c] - b[c]).ravel()) / den)
-    return float(max(errs))
+        err = np.linalg.norm((a[c] - b[c]).ravel())
+        nb = np.linalg.norm(b[c].ravel())
+        own.append(float(err / max(nb, 1e-300)))
+        f = 0.0 if floor is None else float(floor[c])
+        fl.append(float(err / max(nb, f, 1e-300)))
+    return own, fl
+
+
+def field_rel_l2(a, b, floor=None):
+    """Largest per-field relative L2 error, each field against the larger of
+    its own norm and its natural scale ``floor[c]`` (no floor by default)."""
+    return max(field_errors(a, b, floor)[1])
+
+
+def assert_fields_close(a, b, tol, floor=None, what="field"):
+    """Every field within *tol* (against its own norm, or its natural scale
+    where *floor* is given); the message lists both errors per field."""
+    own, fl = field_errors(a, b, floor)
+    bad = [c for c in range(len(fl)) if not fl[c] < tol]
+    msg = "; ".join(f"{what} {c}: own {own[c]:.2e} scaled {fl[c]:.2e}" for c in range(len(fl)))
+    assert not bad, f"fields {bad} above {tol:g}: {msg}"
 
 
 def make_disc(kind, dim, n, order, lo, hi, periodic):
@@ -86,15 +104,7 @@ def perturbed_state_np(x, dim, nspecies, seed=0):
 
 def per_field_rel_l2(a, b, floor=None):
     """Per-field relative L2 errors (same normalisation as field_rel_l2)."""
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
-    big = max(np.linalg.norm(b[c].ravel()) for c in range(b.shape[0]))
-    out = []
-    for c in range(b.shape[0]):
-        fl = 1e-3 * big if floor is None else floor[c]
-        den = max(np.linalg.norm(b[c].ravel()), fl, 1e-300)
-        out.append(float(np.linalg.norm((a[c] - b[c]).ravel()) / den))
-    return out
+    return field_errors(a, b, floor)[1]
 
 
 def flux_scale_floor(q, dim, h, gamma=1.4):
@@ -103,5 +113,41 @@ def flux_scale_floor(q, dim, h, gamma=1.4):
     below its fluxes and roundoff scales with the fluxes)."""
     from oracle import physics as oph
     st = oph.make_fluid_state(q, oph.IdealGas(gamma=gamma), None, dim)
+    return state_flux_floor(st, h)
+
+
+def state_flux_floor(st, h):
+    """|F_c| / h per conserved field for an oracle fluid state *st* (any gas:
+    ideal or mixture), F the inviscid flux."""
+    from oracle import physics as oph
     f = oph.inviscid_flux(st)
-    return [np.linalg.norm(f[c]) / h for c in range(q.shape[0])]
+    return [np.linalg.norm(f[c]) / h for c in range(f.shape[0])]
+
+
+def gradient_floor(q, h):
+    """|q_c| / h per field: the natural scale of a gradient of q_c."""
+    q = np.asarray(q)
+    return [np.linalg.norm(q[c]) / h for c in range(q.shape[0])]
+
+
+def inviscid_flux_floor(q, dim, h, temperature=None, mech=None, gamma=1.4):
+    """|F_c| / h per conserved field from the state alone (numpy, no
+    oracle): F the inviscid flux, the pressure of the ideal gas (gamma) or,
+    with *temperature* and *mech*, of the mixture (p = rho R_u T sum Y_k/W_k)."""
+    q = np.asarray(q, dtype=np.float64)
+    rho = q[0]
+    v = q[2:2 + dim] / rho
+    if mech is None:
+        p = (gamma - 1) * (q[1] - 0.5 * np.sum(q[2:2 + dim] * v, axis=0))
+    else:
+        from mirgecom_b200.thermochemistry import GAS_CONSTANT
+        w = np.asarray(mech.molecular_weights).reshape((-1,) + (1,) * (q.ndim - 1))
+        p = GAS_CONSTANT * np.asarray(temperature) * np.sum(q[2 + dim:] / w, axis=0)
+    out = [np.linalg.norm(q[0] * v), np.linalg.norm((q[1] + p) * v)]
+    for i in range(dim):
+        fi = q[2 + i] * v
+        fi[i] = fi[i] + p
+        out.append(np.linalg.norm(fi))
+    for k in range(q.shape[0] - 2 - dim):
+        out.append(np.linalg.norm(q[2 + dim + k] * v))
+    return [x / h for x in out]

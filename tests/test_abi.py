@@ -48,7 +48,8 @@ def test_invalid_arguments_rejected_without_gpu():
 
 _QUERIES = {"mgc_version", "mgc_supports", "mgc_supports_hex", "mgc_mlp_nparams",
             "mgc_rhs_split_workspace_bytes", "mgc_mlp_train_workspace_bytes",
-            "mgc_ns_operator_noalloc_capacity"}
+            "mgc_ns_operator_noalloc_capacity", "mgc_fp64_probe_flops",
+            "mgc_operator_workspace_bytes"}
 
 
 def _null_call_script():
@@ -94,3 +95,49 @@ def test_every_entry_point_rejects_null_arguments():
     assert set(codes) == set(_lib.exported_symbols()) - _QUERIES
     bad = {k: v for k, v in codes.items() if v >= 0}
     assert not bad, bad
+
+
+def test_noalloc_capacity_edge_without_gpu():
+    """The allocation-free NS entry point accepts a mesh whose gradient
+    buffer fills its fixed array exactly and rejects one element more
+    (MGC_E_TOO_LARGE), checked before any device work: the child process
+    sees no GPU, so the accepted size stops at the device lookup
+    (MGC_E_CUDA) and nothing is launched."""
+    import json
+    import subprocess
+    import sys
+    script = r'''
+import ctypes as C, json, sys
+sys.path.insert(0, %r)
+from mirgecom_b200 import _lib
+lib = _lib.load()
+cap = lib.mgc_ns_operator_noalloc_capacity()
+gas = _lib.GasStruct()
+gas.eos_kind = _lib.EOS_IDEAL
+gas.nspecies = 0
+mesh = _lib.MeshStruct()
+mesh.dim, mesh.order, mesh.elem_kind = 3, 3, 0
+per_elem = (3 + 2 + 1) * 3 * 20          # (Nc+1) * dim * Np doubles per element
+out = {}
+for key, nel in (("edge", cap // per_elem), ("over", cap // per_elem + 1)):
+    mesh.nelem = nel
+    out[key] = lib.mgc_ns_operator_noalloc(C.byref(mesh), C.byref(gas), None, None, None,
+                                           None, 0, 0, None, None, None)
+bad = _lib.MeshStruct()
+bad.dim, bad.order, bad.elem_kind, bad.nelem = 3, 3, 7, 10
+out["bad_kind"] = lib.mgc_ns_operator_noalloc(C.byref(bad), C.byref(gas), None, None, None,
+                                              None, 0, 0, None, None, None)
+bad.elem_kind, bad.order = 0, 1 << 20
+out["huge_order"] = lib.mgc_ns_operator_noalloc(C.byref(bad), C.byref(gas), None, None,
+                                                None, None, 0, 0, None, None, None)
+print(json.dumps(out))
+''' % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),)
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    res = subprocess.run([sys.executable, "-c", script], capture_output=True, text=True,
+                         timeout=120, env=env)
+    assert res.returncode == 0, res.stderr[-2000:]
+    codes = json.loads(res.stdout.strip().splitlines()[-1])
+    assert codes["edge"] == -4, codes          # past the size check, no device
+    assert codes["over"] == -5, codes          # MGC_E_TOO_LARGE
+    assert codes["bad_kind"] == -1, codes      # invalid element kind
+    assert codes["huge_order"] == -2, codes    # unsupported order, no overflow

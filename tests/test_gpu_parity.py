@@ -10,8 +10,8 @@ import numpy as np
 import pytest
 import torch
 
-from cases import (field_rel_l2, flux_scale_floor, make_disc, perturbed_state_np,
-                   rel_l2, tgv_np, vortex_np)
+from cases import (assert_fields_close, field_rel_l2, flux_scale_floor, inviscid_flux_floor,
+                   make_disc, perturbed_state_np, rel_l2, tgv_np, vortex_np)
 from mirgecom_b200 import runtime
 from mirgecom_b200.boundary import DummyBoundary, PrescribedFluidBoundary
 from mirgecom_b200.eos import IdealSingleGas, PyrometheusMixture
@@ -60,8 +60,7 @@ def test_euler_vortex_config1(cuda, flux):
     ref = odg.euler_operator(od, ost, oph.IdealGas(),
                              {"all": odg.PrescribedBoundary(lambda x, tt: vortex_np(x, t=tt))},
                              time=t, flux=flux)
-    err = field_rel_l2(rhs.q.cpu().numpy(), ref)
-    assert err < TOL, err
+    assert_fields_close(rhs.q.cpu().numpy(), ref, TOL)
     _status_ok(d)
 
 
@@ -75,7 +74,7 @@ def test_euler_periodic_species(cuda, dim, order):
                          inviscid_numerical_flux_func=inviscid_facial_flux_rusanov)
     ref = odg.euler_operator(od, oph.make_fluid_state(q, oph.IdealGas(), None, dim),
                              oph.IdealGas(), {}, flux="rusanov")
-    assert field_rel_l2(rhs.q.cpu().numpy(), ref) < TOL
+    assert_fields_close(rhs.q.cpu().numpy(), ref, TOL)
 
 
 def test_ns_taylor_green_config2_small(cuda):
@@ -129,7 +128,9 @@ def test_ns_2d_boundaries_species(cuda, flux):
     ref = odg.ns_operator(od, oph.make_fluid_state(q, oph.IdealGas(), otr, 2),
                           oph.IdealGas(), otr, obnds, flux=flux)
     del qext
-    assert field_rel_l2(rhs.q.cpu().numpy(), ref) < TOL
+    # measured against each field's own norm, or its flux scale |F_c|/h with
+    # h the smaller cell edge (0.2) where that is larger
+    assert_fields_close(rhs.q.cpu().numpy(), ref, TOL, floor=inviscid_flux_floor(q, 2, 0.2))
     _status_ok(d)
 
 
@@ -155,7 +156,12 @@ def test_ns_reacting_mixture(cuda, order):
     assert rel_l2(st.temperature.cpu().numpy(), ost["temperature"]) < 1e-14
     ref = odg.ns_operator(od, ost, ogas, otr, {})
     ref = ref + oph.species_source_terms(ogas, q, ost["temperature"], 3)
-    assert field_rel_l2(rhs.q.cpu().numpy(), ref) < TOL
+    # each field against its own norm, or its inviscid flux scale |F_c|/h
+    # (h the cube edge) where that is larger: only the low-Mach momentum
+    # fields, whose RHS is ~15x below their pressure flux, take the latter
+    floor = inviscid_flux_floor(q, 3, 2 * np.pi / 3, temperature=ost["temperature"],
+                                mech=UIUC_7SP)
+    assert_fields_close(rhs.q.cpu().numpy(), ref, TOL, floor=floor)
     _status_ok(d)
 
 
@@ -206,8 +212,9 @@ def test_uniform_state_rhs_zero(cuda, dim):
 
 
 @pytest.mark.parametrize("case", ["tgv", "mixture", "boundaries_hll"])
-def test_split_and_fused_divergence_agree(cuda, case):
-    """The two-kernel (flux records + surface) and fused divergence passes."""
+def test_rhs_paths_agree(cuda, case):
+    """The volume/face path, the split divergence (flux records + surface) and
+    the fused divergence pass give the same right-hand side."""
     if case == "tgv":
         d, od = make_disc("simplex", 3, 3, 3, (-np.pi,) * 3, (np.pi,) * 3, True)
         q = tgv_np(od.nodes)
@@ -216,6 +223,7 @@ def test_split_and_fused_divergence_agree(cuda, case):
             viscosity=mu, thermal_conductivity=mu * 1004.85 / 0.71))
         st = make_fluid_state(_cv(q, 3, cuda), gas)
         kw, bnds, flux = {}, {}, inviscid_facial_flux_rusanov
+        floor = inviscid_flux_floor(q, 3, 2 * np.pi / 3)
     elif case == "mixture":
         d, od = make_disc("simplex", 3, 3, 3, (0.0,) * 3, (2 * np.pi,) * 3, True)
         from mirgecom_b200.initializers import reacting_mixture_state
@@ -227,6 +235,8 @@ def test_split_and_fused_divergence_agree(cuda, case):
                               temperature_seed=t_true.to(cuda) + 10.0)
         kw, bnds, flux = {"species_source_temperature": st.temperature}, {}, \
             inviscid_facial_flux_rusanov
+        floor = inviscid_flux_floor(cv0.q.numpy(), 3, 2 * np.pi / 3,
+                                    temperature=st.temperature.cpu().numpy(), mech=UIUC_7SP)
     else:
         d, od = make_disc("simplex", 2, 5, 2, (0.0, 0.0), (2.0, 1.0), False)
         q = perturbed_state_np(od.nodes, 2, 2, seed=3)
@@ -241,13 +251,15 @@ def test_split_and_fused_divergence_agree(cuda, case):
                 "-1": PrescribedFluidBoundary(boundary_state_func=bnd), "+1": DummyBoundary()}
         st = make_fluid_state(_cv(q, 2, cuda), gas)
         kw, flux = {}, inviscid_facial_flux_hll
+        floor = inviscid_flux_floor(q, 2, 0.2)
     outs = {}
-    for split in (True, False):
-        runtime.SPLIT_RHS = split
+    for path in ("volume_face", "split", "fused"):
+        runtime.RHS_PATH = path
         try:
-            outs[split] = ns_operator(d, gas, st, bnds, inviscid_numerical_flux_func=flux,
-                                      **kw).q.cpu().numpy()
+            outs[path] = ns_operator(d, gas, st, bnds, inviscid_numerical_flux_func=flux,
+                                     **kw).q.cpu().numpy()
         finally:
-            runtime.SPLIT_RHS = True
-    assert field_rel_l2(outs[True], outs[False]) < TOL
+            runtime.RHS_PATH = "volume_face"
+    assert_fields_close(outs["split"], outs["fused"], TOL, floor=floor)
+    assert_fields_close(outs["volume_face"], outs["fused"], TOL, floor=floor)
     _status_ok(d)

@@ -1,9 +1,11 @@
-"""Adiabatic slip wall, inviscid part (mirgecom/boundary.py:1052-1080).
+"""Adiabatic slip wall in the Euler operator (mirgecom/boundary.py:1052-1080).
 
 CPU: the oracle's Euler RHS of a gas at rest in a closed box of slip walls
 vanishes (a steady state), and the product refuses the viscous operator with
-this wall.  GPU: the device Euler RHS with slip walls on some sides and
-prescribed states on the others matches the oracle at the float64 bar."""
+this wall on hexahedra.  GPU: the device Euler RHS with slip walls on some
+sides and prescribed states on the others matches the oracle at the float64
+bar (simplices: the device slip treatment; hexahedra: its state_plus
+prescribed).  The viscous walls are tested in tests/test_gpu_walls.py."""
 
 import numpy as np
 import pytest
@@ -34,13 +36,15 @@ def test_oracle_rest_state_in_slip_box_is_steady(kind, dim, order):
         assert np.abs(rhs).max() < 1e-10, flux
 
 
-def test_ns_operator_refuses_slip_wall():
+def test_ns_operator_refuses_slip_wall_on_hexahedra():
+    """The viscous slip wall runs on the simplex kernels' volume/face path;
+    the tensor-product hexahedra evaluate only its inviscid part."""
     from mirgecom_b200.navierstokes import ns_operator
     from mirgecom_b200.transport import SimpleTransport
-    d, od = make_disc("simplex", 2, 3, 1, (0.0, 0.0), (1.0, 1.0), False)
+    d, od = make_disc("hypercube", 3, 3, 2, (0.0,) * 3, (1.0,) * 3, False)
     gas = GasModel(eos=IdealSingleGas(), transport=SimpleTransport(viscosity=1e-3))
-    q = perturbed_state_np(od.nodes, 2, 0, seed=1)
-    st = make_fluid_state(ConservedVars(torch.from_numpy(q), 2), gas)
+    q = perturbed_state_np(od.nodes, 3, 0, seed=1)
+    st = make_fluid_state(ConservedVars(torch.from_numpy(q), 3), gas)
     with pytest.raises(NotImplementedError):
         ns_operator(d, gas, st, {"all": AdiabaticSlipBoundary()})
 
