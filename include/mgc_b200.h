@@ -107,6 +107,10 @@ typedef struct {
   const float* rx32;        /* float32 copy of rx, for the *_f32 entry points */
   const uint8_t* fslot;     /* [nperm][Nfp] neighbour face slot fn*Nfp + m' of own face
                                node m (mgc_operator*; may be NULL for the others) */
+  int32_t nowned;           /* mgc_operator*: elements [0, nowned) are evaluated, the
+                               rest are ghost elements of a mesh partition (neighbours
+                               only); 0 = all nelem */
+  int32_t pad_;
 } mgc_mesh_t;
 
 /* Library version and the list of supported (dim, order) pairs. */
@@ -253,19 +257,26 @@ int mgc_rhs_split_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas,
  * needs fslot.  workspace: 256-byte aligned, at least
  * mgc_operator_workspace_bytes(mesh, gas, single_precision) bytes (face-node
  * records [E][Nf][Nfp][round_up(Nc+4, 4)], node-0 fluxes [E][Nf][Nc],
- * boundary records).  mid_event: a cudaEvent_t recorded between the two
- * kernels, or NULL.  Hexahedral meshes return MGC_E_UNSUPPORTED (use
- * mgc_ns_grad* + mgc_rhs_split*). ---- */
+ * boundary records, boundary plus states).  mid_event: a cudaEvent_t
+ * recorded between the two kernels, or NULL.  phases: 1 the volume kernel
+ * only, 2 the face kernel only, 3 both (a partitioned mesh exchanges the
+ * ghost elements' face-node records between the two).  With
+ * mesh->nowned > 0 only elements [0, nowned) are evaluated; elements
+ * [nowned, nelem) are ghosts (q, temperatures and, before the face kernel,
+ * their face-node records filled by the caller's halo exchange).  Hexahedral
+ * meshes return MGC_E_UNSUPPORTED (use mgc_ns_grad* + mgc_rhs_split*). ---- */
 size_t mgc_operator_workspace_bytes(const mgc_mesh_t* mesh, const mgc_gas_t* gas,
                                     int single_precision);
 int mgc_operator(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
                  const double* t_op, const double* t_src, const double* bext, int flux_kind,
                  int add_sources, double* rhs, double* grad_out, void* workspace,
-                 size_t workspace_bytes, int32_t* status, void* stream, void* mid_event);
+                 size_t workspace_bytes, int32_t* status, void* stream, void* mid_event,
+                 int phases);
 int mgc_operator_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
                      const float* t_op, const float* t_src, const float* bext, int flux_kind,
                      int add_sources, float* rhs, float* grad_out, void* workspace,
-                     size_t workspace_bytes, int32_t* status, void* stream, void* mid_event);
+                     size_t workspace_bytes, int32_t* status, void* stream, void* mid_event,
+                     int phases);
 
 /* ---- learned initial guess of the mixture temperature (no counterpart in
  * the reference, whose Newton solve always starts from the seed): an

@@ -64,6 +64,7 @@ class MeshStruct(C.Structure):
         ("nbf", C.c_int32), ("nperm", C.c_int32), ("elem_kind", C.c_int32),
         ("rx", C.c_void_p), ("conn", C.c_void_p), ("perm", C.c_void_p),
         ("bkind", C.c_void_p), ("rx32", C.c_void_p), ("fslot", C.c_void_p),
+        ("nowned", C.c_int32), ("pad_", C.c_int32),
     ]
 
 
@@ -114,9 +115,9 @@ _SIGNATURES = {
         [_P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P], C.c_int),
     "mgc_operator_workspace_bytes": ([_P, _P, C.c_int], C.c_size_t),
     "mgc_operator": ([C.c_int, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P,
-                      C.c_size_t, _P, _P, _P], C.c_int),
+                      C.c_size_t, _P, _P, _P, C.c_int], C.c_int),
     "mgc_operator_f32": ([C.c_int, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int, _P, _P, _P,
-                          C.c_size_t, _P, _P, _P], C.c_int),
+                          C.c_size_t, _P, _P, _P, C.c_int], C.c_int),
     "mgc_fp64_probe_flops": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_double),
     "mgc_fp64_probe": ([C.c_int, C.c_int, C.c_int, C.c_int, _P, _P], C.c_int),
 }

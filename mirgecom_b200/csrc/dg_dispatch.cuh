@@ -149,28 +149,34 @@ struct Launch {
     return ((size_t)nelem * C::NP * C::FW + (size_t)NS * nelem * C::NP) * sizeof(R) + 256;
   }
   // volume kernel then face kernel (dg_volume.cuh)
+  // phases: bit 0 the volume kernel, bit 1 the face kernel
   template <bool VISC>
-  static int vol_face(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
+  static int vol_face(const DGArgs<R>& a, const GasParams& g, cudaStream_t s, int phases) {
     using V = VCfg<R, DIM, ORDER, NS, MIX>;
-    const size_t smem1 = V::vol_bytes(V::EPB, a.nperm);
-    auto k1 = k_volume<R, DIM, ORDER, NS, MIX, VISC>;
-    int rc = prepare_kernel(k1, smem1);
-    if (rc) return rc;
-    int nblk = 0;
-    rc = persistent_grid(k1, V::NT, smem1, (a.nelem + V::EPB - 1) / V::EPB, &nblk);
-    if (rc) return rc;
-    k1<<<nblk, V::NT, smem1, s>>>(a, g);
-    if (cudaGetLastError() != cudaSuccess) return MGC_E_CUDA;
+    int nblk = 0, rc = MGC_OK;
+    if (phases & 1) {
+      const size_t smem1 = V::vol_bytes(V::EPB, a.nperm);
+      auto k1 = k_volume<R, DIM, ORDER, NS, MIX, VISC>;
+      rc = prepare_kernel(k1, smem1);
+      if (rc) return rc;
+      rc = persistent_grid(k1, V::NT, smem1, (a.nowned + V::EPB - 1) / V::EPB, &nblk);
+      if (rc) return rc;
+      k1<<<nblk, V::NT, smem1, s>>>(a, g);
+      if (cudaGetLastError() != cudaSuccess) return MGC_E_CUDA;
+    }
     if (a.mid_event && cudaEventRecord(static_cast<cudaEvent_t>(a.mid_event), s) != cudaSuccess)
       return MGC_E_CUDA;
-    const size_t smem2 = V::face_bytes(a.nperm);
-    auto k2 = k_face<R, DIM, ORDER, NS, MIX, VISC>;
-    rc = prepare_kernel(k2, smem2);
-    if (rc) return rc;
-    rc = persistent_grid(k2, V::NT2, smem2, (a.nelem + V::EPB2 - 1) / V::EPB2, &nblk);
-    if (rc) return rc;
-    k2<<<nblk, V::NT2, smem2, s>>>(a, g);
-    return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+    if (phases & 2) {
+      const size_t smem2 = V::face_bytes(a.nperm);
+      auto k2 = k_face<R, DIM, ORDER, NS, MIX, VISC>;
+      rc = prepare_kernel(k2, smem2);
+      if (rc) return rc;
+      rc = persistent_grid(k2, V::NT2, smem2, (a.nowned + V::EPB2 - 1) / V::EPB2, &nblk);
+      if (rc) return rc;
+      k2<<<nblk, V::NT2, smem2, s>>>(a, g);
+      if (cudaGetLastError() != cudaSuccess) return MGC_E_CUDA;
+    }
+    return MGC_OK;
   }
   // workspace of vol_face: face-node records, node-0 shifts, boundary
   // records, boundary plus states, each 256-byte aligned
@@ -212,8 +218,12 @@ inline int dispatch_order(int op, int ns, bool mix, const DGArgs<R>& a, const Ga
     if (op == 2) return L::template rhs<true>(a, g, s);                  \
     if (op == 3) return L::template rhs_split<false>(a, g, s);           \
     if (op == 4) return L::template rhs_split<true>(a, g, s);            \
-    if (op == 5) return L::template vol_face<false>(a, g, s);            \
-    return L::template vol_face<true>(a, g, s);                          \
+    if (op == 5) return L::template vol_face<false>(a, g, s, 3);         \
+    if (op == 6) return L::template vol_face<true>(a, g, s, 3);          \
+    if (op == 7) return L::template vol_face<false>(a, g, s, 1);         \
+    if (op == 8) return L::template vol_face<true>(a, g, s, 1);          \
+    if (op == 9) return L::template vol_face<false>(a, g, s, 2);         \
+    return L::template vol_face<true>(a, g, s, 2);                       \
   }
   if constexpr (sizeof(R) == 8) {
     MGC_CASE(0, false)

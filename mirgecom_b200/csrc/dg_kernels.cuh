@@ -63,6 +63,9 @@ struct DGArgs {
   R* bplus;            // [NC][nbf][NFP] exterior q of the inviscid flux at boundary faces
   const uint8_t* fslot;  // [nperm][NFP] neighbour face slot fn * NFP + m'
   R* grad_out;         // optional [NC+1][DIM][E][NP] gradients (return_gradients)
+  int32_t nowned;      // elements [0, nowned) are evaluated; the rest (up to nelem)
+                       // are ghosts of a mesh partition, read as neighbours only
+  int32_t pad2_;
 };
 
 // Boundary face kinds (int8 per boundary face).  Prescribed: exterior state

@@ -357,11 +357,11 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT),
   const int gq = lane >> 2, tq = lane & 3;
   const int nwarps = blockDim.x >> 5;
   constexpr int NACC = V::TF32 ? 4 : 2;
-  const int ntiles = (E + EPB - 1) / EPB;
+  const int ntiles = (a.nowned + EPB - 1) / EPB;
   bool bad = false;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = tile * EPB;
-    const int ne = imin(EPB, E - e0);
+    const int ne = imin(EPB, a.nowned - e0);
     // the previous tile's last phase reads the work region, src_s and the
     // geometry, which this tile overwrites
     __syncthreads();
@@ -583,16 +583,12 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT),
 #pragma unroll
         for (int j = 0; j < DIM; ++j) fl[c][j] = -fl[c][j];
       if constexpr (VISC) {
-        R gqv[NC][DIM], gt[DIM];
+        // the gradients are read from the node's shared-memory row where the
+        // viscous flux uses them (no register copy of all (NC+1) DIM values)
         const R* gr = gn + n * GST;
-#pragma unroll
-        for (int c = 0; c < NC; ++c)
-#pragma unroll
-          for (int j = 0; j < DIM; ++j) gqv[c][j] = gr[c * DIM + j];
-#pragma unroll
-        for (int j = 0; j < DIM; ++j) gt[j] = gr[NC * DIM + j];
         R fv[NC][DIM];
-        viscous_flux<R, DIM, NS, MIX>(st, gqv, gt, fv);
+        viscous_flux<R, DIM, NS, MIX>(st, reinterpret_cast<const R(*)[DIM]>(gr), gr + NC * DIM,
+                                      fv);
 #pragma unroll
         for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -827,12 +823,12 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT2),
   const int gq = lane >> 2, tq = lane & 3;
   const int nwarps = blockDim.x >> 5;
   constexpr int NACC = V::TF32 ? 4 : 2;
-  const int ntiles = (E + EPB - 1) / EPB;
+  const int ntiles = (a.nowned + EPB - 1) / EPB;
   const int64_t bstride = (int64_t)a.nbf * NFP;
   bool bad = false;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = tile * EPB;
-    const int ne = imin(EPB, E - e0);
+    const int ne = imin(EPB, a.nowned - e0);
     // (the previous tile's contraction reads am / bm only; load_geometry's
     // first barrier orders it before this tile's writes of bm)
     stage_conn<NF>(a.conn, e0, ne, conn_s);

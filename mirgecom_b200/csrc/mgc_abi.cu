@@ -252,7 +252,8 @@ template <class R>
 int operator_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const R* q,
                   const R* t_op, const R* t_src, const R* bext, int flux_kind, int add_sources,
                   R* rhs, R* grad_out, void* workspace, size_t workspace_bytes, int32_t* status,
-                  void* stream, void* mid_event) {
+                  void* stream, void* mid_event, int phases) {
+  if (phases < 1 || phases > 3) return MGC_E_INVALID;
   if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !rhs || !status || !workspace)
     return MGC_E_INVALID;
   if (flux_kind < 0 || flux_kind > 2) return MGC_E_INVALID;
@@ -261,6 +262,7 @@ int operator_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const 
   if (grad_out && !visc) return MGC_E_INVALID;
   if (mesh->elem_kind != kElemSimplex) return MGC_E_UNSUPPORTED;
   if (!mesh->fslot) return MGC_E_INVALID;
+  if (mesh->nowned < 0 || mesh->nowned > mesh->nelem) return MGC_E_INVALID;
   if (reinterpret_cast<uintptr_t>(workspace) % 256) return MGC_E_INVALID;
   int rc = ready(mesh, gas);
   if (rc) return rc;
@@ -278,7 +280,9 @@ int operator_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const 
   a.fslot = mesh->fslot;
   a.grad_out = grad_out;
   a.mid_event = mid_event;
-  return dispatch(visc ? 6 : 5, mesh, gas, a, (cudaStream_t)stream);
+  a.nowned = mesh->nowned > 0 ? mesh->nowned : mesh->nelem;
+  const int op = (phases == 3) ? 5 : (phases == 1 ? 7 : 9);
+  return dispatch(op + (visc ? 1 : 0), mesh, gas, a, (cudaStream_t)stream);
 }
 
 }  // namespace
@@ -295,19 +299,21 @@ size_t mgc_operator_workspace_bytes(const mgc_mesh_t* mesh, const mgc_gas_t* gas
 int mgc_operator(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const double* q,
                  const double* t_op, const double* t_src, const double* bext, int flux_kind,
                  int add_sources, double* rhs, double* grad_out, void* workspace,
-                 size_t workspace_bytes, int32_t* status, void* stream, void* mid_event) {
+                 size_t workspace_bytes, int32_t* status, void* stream, void* mid_event,
+                 int phases) {
   return operator_impl<double>(viscous, mesh, gas, q, t_op, t_src, bext, flux_kind, add_sources,
                                rhs, grad_out, workspace, workspace_bytes, status, stream,
-                               mid_event);
+                               mid_event, phases);
 }
 
 int mgc_operator_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const float* q,
                      const float* t_op, const float* t_src, const float* bext, int flux_kind,
                      int add_sources, float* rhs, float* grad_out, void* workspace,
-                     size_t workspace_bytes, int32_t* status, void* stream, void* mid_event) {
+                     size_t workspace_bytes, int32_t* status, void* stream, void* mid_event,
+                     int phases) {
   return operator_impl<float>(viscous, mesh, gas, q, t_op, t_src, bext, flux_kind, add_sources,
                               rhs, grad_out, workspace, workspace_bytes, status, stream,
-                              mid_event);
+                              mid_event, phases);
 }
 
 size_t mgc_rhs_split_workspace_bytes(const mgc_mesh_t* mesh, const mgc_gas_t* gas,

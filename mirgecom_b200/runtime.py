@@ -107,6 +107,8 @@ class DeviceDiscretization:
         self.mesh.bkind = None
         self.mesh.rx32 = self.rx32.data_ptr()
         self.mesh.fslot = self.fslot.data_ptr()
+        # a partition's ghost elements follow its owned ones
+        self.mesh.nowned = int(getattr(dcoll, "nowned", 0))
         self.mesh.elem_kind = 1 if dcoll.refel.kind == "hypercube" else 0
 
     def workspace(self, name, shape, dtype=torch.float64):
@@ -297,11 +299,23 @@ def _operator_workspace(dd, gs, f32):
     return dd.workspace("operator_ws", ((nbytes + 255) // 256 * 256,), torch.uint8)
 
 
+def face_records(dd, gs, f32, nc):
+    """The face-node records [E, Nf, Nfp, TW] in the operator workspace (the
+    first part of its layout), as a tensor view for the halo exchange."""
+    ws = _operator_workspace(dd, gs, f32)
+    dtype = torch.float32 if f32 else torch.float64
+    dc = dd.dcoll
+    tw = -(-(nc + 4) // 4) * 4
+    n = dc.nelements * dc.nfaces * dc.nface_nodes * tw
+    return ws[:n * (4 if f32 else 8)].view(dtype).view(dc.nelements, dc.nfaces,
+                                                        dc.nface_nodes, tw)
+
+
 def _run_operator(viscous, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs, grad_out,
-                  events=None):
-    """mgc_operator*: volume kernel then face kernel.  *events* (3 CUDA
-    events): recorded before the volume kernel, between the two kernels and
-    after the face kernel."""
+                  events=None, phases=3):
+    """mgc_operator*: volume kernel then face kernel (*phases* 1: volume only,
+    2: face only, 3: both).  *events* (3 CUDA events): recorded before the
+    volume kernel, between the two kernels and after the face kernel."""
     lib = _lib.load()
     f32 = q.dtype == torch.float32
     ws = _operator_workspace(dd, gs, f32)
@@ -316,7 +330,7 @@ def _run_operator(viscous, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs
     _lib.check(fn(int(viscous), C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op),
                   _lib.ptr(t_src), _lib.ptr(bext), flux_kind, int(add_src), _lib.ptr(rhs),
                   _lib.ptr(grad_out), _lib.ptr(ws), ws.numel(), _lib.ptr(dd.status),
-                  _lib.stream_handle(), mid), "mgc_operator")
+                  _lib.stream_handle(), mid, int(phases)), "mgc_operator")
     if events:
         events[2].record()
 
@@ -371,14 +385,23 @@ def _check_boundary_path(dcoll, boundaries):
 
 
 def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
-           source_temperature=None, want_gradients=False, events=None):
+           source_temperature=None, want_gradients=False, events=None, halo=None,
+           phases=3, rhs=None):
     """The Navier-Stokes right-hand side; returns (rhs, gradients or None).
     Gradients [Nc+1, dim, E, Np] are returned when *want_gradients* (they are
     only written to HBM then, on the volume/face path).  *events*: on the
     volume/face path 3 CUDA events (before the volume kernel, between the
     two kernels, after the face kernel); on the other paths 3 or 4 (before
     the gradient pass, between the passes, [between the node-flux and surface
-    kernels,] after the divergence)."""
+    kernels,] after the divergence).
+
+    Mesh partitions (*dcoll* a :class:`~mirgecom_b200.partition.
+    PartitionedDiscretization`, the state's ghost rows already exchanged):
+    with *halo* (a :class:`~mirgecom_b200.partition.HaloExchange`) the face
+    records of the ghosts are exchanged between the two kernels; or the
+    caller runs the kernels one at a time (*phases* 1 then 2, passing the
+    first call's *rhs* to the second) and exchanges the records of
+    :func:`face_records` in between."""
     _check_boundary_path(dcoll, boundaries)
     q = state.cv.q
     _lib.require_cuda(q)
@@ -393,7 +416,7 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
     t_op = _operator_temperature(state)
     if source_temperature is not None:
         source_temperature = source_temperature.to(q.dtype)
-    rhs = torch.empty_like(q)
+    rhs = torch.empty_like(q) if rhs is None else rhs
     stream = _lib.stream_handle()
     add_src = source_temperature is not None
     t_src = source_temperature.contiguous() if add_src else None
@@ -403,8 +426,15 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
     if path == "volume_face":
         grad = torch.empty(gshape, dtype=q.dtype, device=q.device) if want_gradients else None
         with torch.cuda.device(q.device):
-            _run_operator(True, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs, grad,
-                          events=events)
+            if halo is None:
+                _run_operator(True, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs, grad,
+                              events=events, phases=phases)
+            else:
+                _run_operator(True, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs, grad,
+                              phases=1)
+                halo.exchange_records(face_records(dd, gs, f32, nc))
+                _run_operator(True, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs, None,
+                              phases=2)
         return rhs, grad
     grad = dd.workspace("grad", gshape, q.dtype)
     fgrad = lib.mgc_ns_grad_f32 if f32 else lib.mgc_ns_grad
