@@ -119,8 +119,26 @@ def build_workload(name, device):
     return dcoll, cv, gas, tseed
 
 
-KERNEL_NAMES = {"state": "k_mixture_state*", "grad": "k_grad", "node_flux": "k_node_flux",
-                "surface": "k_surface", "volume": "k_volume", "face": "k_face"}
+def contraction_flops(dcoll, nc):
+    """Tensor-core flops per launch of the volume and face kernels on
+    simplices (dense reference matrices, inverse mass folded in): volume =
+    the gradient pass (Nc+1) d 2 Np^2 + its lift (Nc+1) 2 Np Nf Nfp, plus the
+    volume divergence Nc d 2 Np^2; face = the lift Nc 2 Np Nf Nfp; per
+    element.  The three-kernel layout splits volume into grad (the gradient
+    pass) and flux_volume (the divergence)."""
+    d = dcoll.dim
+    npn = dcoll.refel.nnodes
+    nfn = dcoll.nfaces * dcoll.nface_nodes
+    e = dcoll.nelements
+    grad = (nc + 1) * d * 2 * npn * npn + (nc + 1) * 2 * npn * nfn
+    div = nc * d * 2 * npn * npn
+    return {"volume": float(e * (grad + div)), "grad": float(e * grad),
+            "flux_volume": float(e * div), "face": float(e * nc * 2 * npn * nfn)}
+
+
+KERNEL_NAMES = {"state": "k_mixture_state*", "grad": "k_grad*", "node_flux": "k_node_flux",
+                "surface": "k_surface", "volume": "k_volume", "flux_volume": "k_flux_volume",
+                "face": "k_face"}
 
 
 def algorithmic_bytes(dcoll, nc, s=8, mixture=False):
@@ -154,6 +172,9 @@ def algorithmic_bytes(dcoll, nc, s=8, mixture=False):
         # from L2 when the element order keeps neighbours close)
         "face": ne * (nfn * tw + dcoll.nfaces * nc) * s + nn * (nc + 2 * nc) * s + geo,
         "grad": nn * (nc + t_in + (nc + 1) * d) * s + geo,
+        # flux-volume: the volume kernel's traffic plus reading the gradients
+        "flux_volume": nn * (nc + t_in * (2 if s == 8 else 1) + nc + (nc + 1) * d) * s
+                       + ne * (nfn * tw + dcoll.nfaces * nc) * s + geo,
         "node_flux": nn * (nc + (nc + 1) * d + 2 * t_in + fw + (ns if mixture else 0)) * s,
         "surface": nn * (fw + nc + (ns if mixture else 0) + nc) * s + geo,
         "rhs": nn * (nc + (nc + 1) * d + nc + 2 * t_in) * s + geo,
@@ -379,7 +400,9 @@ def _time_form(dcoll, gas, q, tseed, steps, warmup, flush, stream):
     import torch
 
     from mirgecom_b200 import runtime
-    vf = runtime._path(dcoll) == "volume_face"
+    path = runtime._path(dcoll)
+    vf = path == "volume_face"
+    three = path == "gradient_volume_face"
     nev = 4 if vf else 5
     for _ in range(warmup):
         _rhs_call(dcoll, gas, q, tseed)
@@ -387,7 +410,8 @@ def _time_form(dcoll, gas, q, tseed, steps, warmup, flush, stream):
     evs = []
     for i in range(steps):
         flush.fill_(float(i))
-        # start | state | volume | face    or    start | state | grad | node_flux | surface
+        # start | state | volume | face,  start | state | grad | flux_volume | face
+        # or  start | state | grad | node_flux | surface
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(nev)]
         _rhs_call(dcoll, gas, q, tseed, events=ev)
         evs.append(ev)
@@ -399,6 +423,9 @@ def _time_form(dcoll, gas, q, tseed, steps, warmup, flush, stream):
     if vf:
         kern = {"state": mean(0, 1), "volume": mean(1, 2), "face": mean(2, 3),
                 "rhs": mean(1, 3)}
+    elif three:
+        kern = {"state": mean(0, 1), "grad": mean(1, 2), "flux_volume": mean(2, 3),
+                "face": mean(3, 4), "rhs": mean(1, 4)}
     else:
         kern = {"state": mean(0, 1), "grad": mean(1, 2), "node_flux": mean(2, 3),
                 "surface": mean(3, 4), "rhs": mean(2, 4)}
@@ -937,6 +964,22 @@ def _run_ours(args):
     achieved = ab[top] / (kt[top] / 1e3) / 1e9
     ab64 = algorithmic_bytes(dcoll, nc, s=8, mixture=mixture)
     k64 = res["plain_fp64"][1]
+    # the float64 path's compute roofline: its contractions run on the
+    # float64 tensor cores (DMMA); the peak is measured here by a probe
+    fp64 = None
+    if "face" in k64 and world == 1:
+        from mirgecom_b200 import fp64_peak
+        pk = fp64_peak.measure(dev)
+        fl = contraction_flops(dcoll, nc)
+        fp64 = {"dmma_peak_tflops": pk["dmma_tflops"], "dfma_peak_tflops": pk["dfma_tflops"],
+                "peak_how": pk["how"], "kernels": {}}
+        for kname in ("volume", "grad", "flux_volume", "face"):
+            if kname not in k64:
+                continue
+            tf = fl[kname] / (k64[kname] / 1e3) / 1e12
+            fp64["kernels"][KERNEL_NAMES[kname]] = {
+                "contraction_flops": fl[kname], "achieved_tflops": tf,
+                "dmma_frac": tf / pk["dmma_tflops"]}
     kt64 = {k: v for k, v in k64.items() if k in ab64 and k != "rhs"}
     top64 = max(kt64, key=kt64.get)
     traffic = traffic64 = None
@@ -953,7 +996,8 @@ def _run_ours(args):
     # this library's kernels per step: temperature (mixtures), gradient, and
     # the divergence pass (node flux + surface on the split path)
     from mirgecom_b200 import runtime as _rt
-    per_step = (1 if mixture else 0) + (2 if _rt._path(dcoll) == "volume_face" else 3)
+    per_step = (1 if mixture else 0) + {"volume_face": 2, "gradient_volume_face": 3}.get(
+        _rt._path(dcoll), 3)
     line = {
         "metric": "DOF-RHS evals/s", "value": values[head], "unit": "DOF-RHS/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -989,7 +1033,8 @@ def _run_ours(args):
         "roofline_plain_fp64": {"kernel": KERNEL_NAMES.get(top64, top64), "phase": top64,
                                 "achieved": ab64[top64] / (kt64[top64] / 1e3) / 1e9,
                                 "frac": ab64[top64] / (kt64[top64] / 1e3) / 1e9 / hbm,
-                                "algorithmic_bytes": ab64[top64], "traffic": traffic64},
+                                "algorithmic_bytes": ab64[top64], "traffic": traffic64,
+                                "compute": fp64},
         "device_status": status,
         "rhs_rel_l2_vs_fp64": rhs_err,
         "end_of_run": eor,
@@ -1020,7 +1065,13 @@ def main(argv=None):
     ap.add_argument("--profile", action="store_true",
                     help="time the plain and mixed forms only (no network training, "
                          "end-to-end or CPU legs): the command profiled with ncu")
+    ap.add_argument("--gradient-kernel", default="auto", choices=["auto", "mma_sync"],
+                    help="gradient-pass kernel: the tcgen05 pipelined kernel where it "
+                         "applies (auto) or the mma.sync kernel")
     args = ap.parse_args(argv)
+    if args.impl != "reference" and args.gradient_kernel != "auto":
+        from mirgecom_b200 import runtime
+        runtime.set_gradient_kernel(args.gradient_kernel)
     if args.impl == "reference":
         run_reference(args)
     elif args.vortex_run:

@@ -44,6 +44,8 @@ extern "C" {
 #define MGC_ST_NAN 1
 #define MGC_ST_BAD_INDEX 2
 #define MGC_ST_NEWTON_MISS 4
+#define MGC_ST_NONPOSITIVE 8
+#define MGC_ST_WAIT_TIMEOUT 16
 
 #define MGC_MAX_SPECIES 16
 #define MGC_MAX_REACTIONS 8
@@ -244,6 +246,19 @@ int mgc_rhs_split_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas,
                       void* workspace, size_t workspace_bytes, int32_t* status, void* stream,
                       void* mid_event);
 
+/* Gradient-pass kernel of every entry point that computes gradients
+ * (mgc_ns_grad*, mgc_ns_rhs*'s callers, mgc_operator* with phases bit 4):
+ * MGC_GRAD_AUTO (default) runs the tcgen05/TMEM pipelined kernel where it
+ * applies (float32, 3-D simplices, mixtures, rows of Np floats in 16-byte
+ * pieces) and the mma.sync kernel elsewhere; MGC_GRAD_MMA_SYNC always runs
+ * the mma.sync kernel.  Process-wide; returns MGC_E_INVALID for other
+ * values.  Replaces no reference interface (the reference has one gradient
+ * code path, grad_operator, mirgecom/navierstokes.py:443-446). */
+#define MGC_GRAD_AUTO 0
+#define MGC_GRAD_MMA_SYNC 1
+int mgc_set_gradient_kernel(int kind);
+int mgc_get_gradient_kernel(void);
+
 /* ---- euler_operator (viscous = 0; mirgecom/euler.py:313-416, non-ESDG
  * branch) or ns_operator (viscous = 1; mirgecom/navierstokes.py:350-575,
  * with return_gradients when grad_out is non-NULL) in one call on
@@ -260,7 +275,11 @@ int mgc_rhs_split_f32(int viscous, const mgc_mesh_t* mesh, const mgc_gas_t* gas,
  * boundary records, boundary plus states).  mid_event: a cudaEvent_t
  * recorded between the two kernels, or NULL.  phases: 1 the volume kernel
  * only, 2 the face kernel only, 3 both (a partitioned mesh exchanges the
- * ghost elements' face-node records between the two).  With
+ * ghost elements' face-node records between the two); | 4 runs the volume
+ * stage as two kernels, the gradient kernel (gradients into grad_out,
+ * required when viscous) then a flux-volume kernel that reads them; | 8
+ * (with 4) skips that gradient kernel: grad_out already holds the
+ * gradients (from mgc_ns_grad*).  With
  * mesh->nowned > 0 only elements [0, nowned) are evaluated; elements
  * [nowned, nelem) are ghosts (q, temperatures and, before the face kernel,
  * their face-node records filled by the caller's halo exchange).  Hexahedral

@@ -120,6 +120,8 @@ _SIGNATURES = {
                           C.c_size_t, _P, _P, _P, C.c_int], C.c_int),
     "mgc_fp64_probe_flops": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_double),
     "mgc_fp64_probe": ([C.c_int, C.c_int, C.c_int, C.c_int, _P, _P], C.c_int),
+    "mgc_set_gradient_kernel": ([C.c_int], C.c_int),
+    "mgc_get_gradient_kernel": ([], C.c_int),
 }
 
 _lib = None

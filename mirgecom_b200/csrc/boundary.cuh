@@ -16,6 +16,27 @@
 
 namespace mgc {
 
+// Boundary face kinds (int8 per boundary face).  Prescribed: exterior state
+// from the caller (boundary.py:796-1009).  The others are the Mengaldo
+// treatment (boundary.py:391-793) with their states computed on the device
+// from the interior trace; their parameters travel in the exterior-state
+// array: the wall temperature in the temperature row (isothermal), the free
+// stream state (far field), the boundary pressure in row 0 (outflow).
+enum BoundaryKind {
+  BK_DUMMY = 0,
+  BK_PRESCRIBED = 1,
+  BK_SLIP = 2,          // AdiabaticSlipBoundary          boundary.py:1052-1143
+  BK_NOSLIP = 3,        // AdiabaticNoslipWallBoundary    boundary.py:1794-1858
+  BK_ISOTHERMAL = 4,    // IsothermalWallBoundary         boundary.py:1727-1792
+  BK_FARFIELD = 5,      // FarfieldBoundary               boundary.py:1146-1228
+  BK_OUTFLOW = 6,       // PressureOutflowBoundary        boundary.py:1231-1403
+};
+__host__ __device__ constexpr bool bk_mengaldo(int k) { return k >= BK_SLIP && k <= BK_OUTFLOW; }
+// kinds whose exterior-state array entries are read
+__host__ __device__ constexpr bool bk_needs_bext(int k) {
+  return k == BK_PRESCRIBED || k == BK_ISOTHERMAL || k == BK_FARFIELD || k == BK_OUTFLOW;
+}
+
 template <class R, int NS>
 __device__ __forceinline__ R bc_internal_energy(const GasParams& g, const R* y, R t) {
   if (g.eos_kind == EOS_IDEAL) return (R)g.gas_const / ((R)g.gamma - R(1)) * t;

@@ -8,6 +8,7 @@
 
 #include "dg_kernels.cuh"
 #include "dg_volume.cuh"
+#include "grad_tc.cuh"
 #include "../../include/mgc_b200.h"
 
 namespace mgc {
@@ -113,7 +114,17 @@ inline int persistent_grid(Kern kern, int threads, size_t smem, int64_t tiles, i
 template <class R, int DIM, int ORDER, int NS, bool MIX>
 struct Launch {
   using C = Cfg<R, DIM, ORDER, NS, MIX>;
+  // the gradient kernel over the owned elements of a partition (its tile
+  // loop runs to nelem): elements [nowned, nelem) are ghosts
+  static int grad_owned(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
+    return grad(a, g, s);
+  }
   static int grad(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
+    if constexpr (sizeof(R) == 4 && MIX && DIM == 3) {
+      if constexpr (TcGrad<DIM, ORDER, NS>::OK) {
+        if (a.grad_kernel == 0 && grad_tc_applies(a)) return grad_tc(a, g, s);
+      }
+    }
     const size_t smem = C::smem_grad(a.nperm);
     auto kern = k_grad<R, DIM, ORDER, NS, MIX>;
     int rc = prepare_kernel(kern, smem);
@@ -123,6 +134,28 @@ struct Launch {
     rc = persistent_grid(kern, C::NT, smem, ntiles, &nblk);
     if (rc) return rc;
     kern<<<nblk, C::NT, smem, s>>>(a, g);
+    return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
+  }
+  // the tcgen05 gradient kernel reads rows of q and T in 16-byte pieces
+  static bool grad_tc_applies(const DGArgs<R>& a) {
+    const uintptr_t al = reinterpret_cast<uintptr_t>(a.q) | reinterpret_cast<uintptr_t>(a.t_op) |
+                         reinterpret_cast<uintptr_t>(a.out);
+    return a.t_op != nullptr && (al & 15) == 0 && a.nperm <= 64;
+  }
+  static int grad_tc(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
+    using T = TcGrad<DIM, ORDER, NS>;
+    const size_t smem = T::smem_bytes(a.nperm);
+    auto kern = k_grad_tc<DIM, ORDER, NS>;
+    int rc = prepare_kernel(kern, smem);
+    if (rc) return rc;
+    const int eown = a.nowned > 0 ? a.nowned : a.nelem;
+    const int ntiles = (eown + T::EPB - 1) / T::EPB;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return MGC_E_CUDA;
+    const int nblk = ntiles < sms ? (ntiles > 0 ? ntiles : 1) : sms;
+    kern<<<nblk, T::NT, smem, s>>>(a, g);
     return cudaGetLastError() == cudaSuccess ? MGC_OK : MGC_E_CUDA;
   }
   template <bool VISC>
@@ -149,12 +182,37 @@ struct Launch {
     return ((size_t)nelem * C::NP * C::FW + (size_t)NS * nelem * C::NP) * sizeof(R) + 256;
   }
   // volume kernel then face kernel (dg_volume.cuh)
-  // phases: bit 0 the volume kernel, bit 1 the face kernel
+  // a.phases: bit 0 the volume stage, bit 1 the face kernel; bit 2 runs the
+  // volume stage as the gradient kernel (gradients into a.grad_out) and the
+  // flux-volume kernel instead of the fused volume kernel; bit 3 (with bit
+  // 2) skips the gradient kernel, a.grad_out holding the gradients already
   template <bool VISC>
-  static int vol_face(const DGArgs<R>& a, const GasParams& g, cudaStream_t s, int phases) {
+  static int vol_face(const DGArgs<R>& a, const GasParams& g, cudaStream_t s) {
     using V = VCfg<R, DIM, ORDER, NS, MIX>;
+    const int phases = a.phases;
     int nblk = 0, rc = MGC_OK;
-    if (phases & 1) {
+    if ((phases & 1) && (phases & 4)) {
+      DGArgs<R> b = a;
+      if (VISC) {
+        // the gradient kernel writes its gradients to ga.out (bit 3: the
+        // caller has computed them)
+        if (!(phases & 8)) {
+          DGArgs<R> ga = a;
+          ga.out = a.grad_out;
+          rc = grad_owned(ga, g, s);
+          if (rc) return rc;
+        }
+        b.grad = a.grad_out;
+      }
+      const size_t smem3 = V::flux_bytes(V::EPB3, a.nperm);
+      auto k3 = k_flux_volume<R, DIM, ORDER, NS, MIX, VISC>;
+      rc = prepare_kernel(k3, smem3);
+      if (rc) return rc;
+      rc = persistent_grid(k3, V::NT3, smem3, (a.nowned + V::EPB3 - 1) / V::EPB3, &nblk);
+      if (rc) return rc;
+      k3<<<nblk, V::NT3, smem3, s>>>(b, g);
+      if (cudaGetLastError() != cudaSuccess) return MGC_E_CUDA;
+    } else if (phases & 1) {
       const size_t smem1 = V::vol_bytes(V::EPB, a.nperm);
       auto k1 = k_volume<R, DIM, ORDER, NS, MIX, VISC>;
       rc = prepare_kernel(k1, smem1);
@@ -218,12 +276,8 @@ inline int dispatch_order(int op, int ns, bool mix, const DGArgs<R>& a, const Ga
     if (op == 2) return L::template rhs<true>(a, g, s);                  \
     if (op == 3) return L::template rhs_split<false>(a, g, s);           \
     if (op == 4) return L::template rhs_split<true>(a, g, s);            \
-    if (op == 5) return L::template vol_face<false>(a, g, s, 3);         \
-    if (op == 6) return L::template vol_face<true>(a, g, s, 3);          \
-    if (op == 7) return L::template vol_face<false>(a, g, s, 1);         \
-    if (op == 8) return L::template vol_face<true>(a, g, s, 1);          \
-    if (op == 9) return L::template vol_face<false>(a, g, s, 2);         \
-    return L::template vol_face<true>(a, g, s, 2);                       \
+    if (op == 5) return L::template vol_face<false>(a, g, s);            \
+    return L::template vol_face<true>(a, g, s);                          \
   }
   if constexpr (sizeof(R) == 8) {
     MGC_CASE(0, false)

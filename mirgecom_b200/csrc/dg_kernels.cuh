@@ -31,6 +31,7 @@
 // there are no atomics and results are deterministic run to run.
 // Device-detected problems go to *status* (bit mask) and never trap.
 #pragma once
+#include "boundary.cuh"
 #include "dg_refops.cuh"
 #include "physics.cuh"
 
@@ -65,30 +66,13 @@ struct DGArgs {
   R* grad_out;         // optional [NC+1][DIM][E][NP] gradients (return_gradients)
   int32_t nowned;      // elements [0, nowned) are evaluated; the rest (up to nelem)
                        // are ghosts of a mesh partition, read as neighbours only
+  int32_t phases;      // volume/face path: bit 0 volume stage, bit 1 face stage,
+                       // bit 2 the volume stage as gradient kernel (into grad_out)
+                       // then flux-volume kernel
+  int32_t grad_kernel; // gradient pass: 0 tcgen05 where it applies, else mma.sync;
+                       // 1 always mma.sync
   int32_t pad2_;
 };
-
-// Boundary face kinds (int8 per boundary face).  Prescribed: exterior state
-// from the caller (boundary.py:796-1009).  The others are the Mengaldo
-// treatment (boundary.py:391-793) with their states computed on the device
-// from the interior trace; their parameters travel in the exterior-state
-// array: the wall temperature in the temperature row (isothermal), the free
-// stream state (far field), the boundary pressure in row 0 (outflow).
-enum BoundaryKind {
-  BK_DUMMY = 0,
-  BK_PRESCRIBED = 1,
-  BK_SLIP = 2,          // AdiabaticSlipBoundary          boundary.py:1052-1143
-  BK_NOSLIP = 3,        // AdiabaticNoslipWallBoundary    boundary.py:1794-1858
-  BK_ISOTHERMAL = 4,    // IsothermalWallBoundary         boundary.py:1727-1792
-  BK_FARFIELD = 5,      // FarfieldBoundary               boundary.py:1146-1228
-  BK_OUTFLOW = 6,       // PressureOutflowBoundary        boundary.py:1231-1403
-};
-__host__ __device__ constexpr bool bk_mengaldo(int k) { return k >= BK_SLIP && k <= BK_OUTFLOW; }
-// kinds whose exterior-state array entries are read
-__host__ __device__ constexpr bool bk_needs_bext(int k) {
-  return k == BK_PRESCRIBED || k == BK_ISOTHERMAL || k == BK_FARFIELD || k == BK_OUTFLOW;
-}
-
 
 __host__ __device__ constexpr int imin(int a, int b) { return a < b ? a : b; }
 __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
@@ -348,6 +332,40 @@ __device__ __forceinline__ void stage_conn(const int32_t* __restrict__ conn_g, i
     conn_s[idx] = conn_g[(int64_t)e0 * NF + idx];
 }
 
+// Interior state of a boundary face node: q- from HBM, the operator
+// temperature (mixtures) or the ideal gas's, and p, c, gamma.
+template <class R, int DIM, int NS, bool MIX>
+__device__ __forceinline__ void boundary_minus(const DGArgs<R>& a, const GasParams& g, int64_t EN,
+                                               int64_t gm, R* qm, NodeState<R, DIM, NS>& sm) {
+  constexpr int NC = DIM + 2 + NS;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) qm[c] = a.q[c * EN + gm];
+  make_state<R, DIM, NS>(qm, MIX ? a.t_op[gm] : R(0), g, sm);
+}
+
+// The gradient pass's face value at a Mengaldo boundary face node:
+// (state_bc.cv, temperature_bc) into up[NC + 1] (boundary.py:732-793).
+template <class R, int DIM, int NS, bool MIX>
+__device__ __noinline__ void mengaldo_grad_value(const DGArgs<R> a, const GasParams g, int kind,
+                                                 int bf, int m, int nfp, int64_t EN, int64_t gm,
+                                                 R n0, R n1, R n2, R* up) {
+  constexpr int NC = DIM + 2 + NS;
+  const R n[3] = {n0, n1, n2};
+  R qm[NC];
+  NodeState<R, DIM, NS> sm;
+  boundary_minus<R, DIM, NS, MIX>(a, g, EN, gm, qm, sm);
+  R par[NC + 1];
+  const int64_t bstride = (int64_t)a.nbf * nfp, bo = (int64_t)bf * nfp + m;
+#pragma unroll
+  for (int c = 0; c <= NC; ++c) par[c] = bk_needs_bext(kind) ? a.bext[c * bstride + bo] : R(0);
+  R qbc[NC];
+  const R tbc = bc_state_cv<R, DIM, NS>(kind, g, qm, sm.t, sm.p, sm.c, sm.gamma, n, par, qbc);
+#pragma unroll
+  for (int c = 0; c < NC; ++c) up[c] = qbc[c];
+  up[NC] = tbc;
+}
+
+
 // {{{ mixture temperature
 
 // plain form: T1 = Newton(seed), T2 = Newton(T1), fixed iteration count.
@@ -489,10 +507,12 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
   const int gq = lane >> 2, tq = lane & 3;
   const int nwarps = blockDim.x >> 5;
   constexpr int NACC = C::TF32 ? 4 : 2;     // accumulator entries per lane per m-tile
-  const int ntiles = (E + EPB - 1) / EPB;
+  // elements [0, nowned) of a partition (0: all)
+  const int EOWN = a.nowned > 0 ? a.nowned : E;
+  const int ntiles = (EOWN + EPB - 1) / EPB;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = tile * EPB;
-    const int ne = imin(EPB, E - e0);
+    const int ne = imin(EPB, EOWN - e0);
     // the previous tile's phase 3 reads rx_s and nrm_s, which load_geometry
     // overwrites before its own first barrier
     __syncthreads();
@@ -552,7 +572,8 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
       const int k = fn_s[fm];
       const int cn = conn_s[e * NF + f];
       const R fsc = fs_s[e * NF + f];
-      // 0: two-sided average with node gi; 1: prescribed exterior; 2: interior value
+      // 0: two-sided average with node gi; 1: prescribed exterior; 2: interior
+      // value; 3: Mengaldo boundary state (becomes 1)
       int mode = 2;
       int64_t gi = 0;
       int bf = 0;
@@ -567,11 +588,13 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
         }
       } else {
         bf = -(cn + 1);
-        const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
+        int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
+        if ((bk_needs_bext(kind) && !a.bext) || kind > BK_OUTFLOW) kind = -1;
         if (kind == BK_PRESCRIBED) {
           mode = 1;
-        } else if (kind != BK_DUMMY) {
-          // unknown kind, or one only the volume/face path evaluates
+        } else if (bk_mengaldo(kind)) {
+          mode = 3;
+        } else if (kind < 0) {
           atomicOr(a.status, ST_BAD_INDEX);
         }
       }
@@ -583,12 +606,21 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
       }
       const int64_t bstride = (int64_t)a.nbf * NFP, bo = (int64_t)bf * NFP + m;
       R up[NU];
+      if (mode == 3) {
+        const R* nf = nrm_s + (e * NF + f) * DIM;
+        mengaldo_grad_value<R, DIM, NS, MIX>(a, g, a.bkind[bf], bf, m, NFP, EN,
+                                             (int64_t)(e0 + e) * NP + k, nf[0], nf[1],
+                                             DIM > 2 ? nf[DIM - 1] : R(0), up);
+        mode = 1;
+      } else {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) up[c] = (mode == 0) ? a.q[c * EN + gi] : a.bext[c * bstride + bo];
-      if (MIX)
-        up[NC] = (mode == 0) ? a.t_op[gi] : a.bext[NC * bstride + bo];
-      else
-        up[NC] = node_temperature<R, DIM, NS>(up, R(0), g);
+        for (int c = 0; c < NC; ++c)
+          up[c] = (mode == 0) ? a.q[c * EN + gi] : a.bext[c * bstride + bo];
+        if (MIX)
+          up[NC] = (mode == 0) ? a.t_op[gi] : a.bext[NC * bstride + bo];
+        else
+          up[NC] = node_temperature<R, DIM, NS>(up, R(0), g);
+      }
 #pragma unroll
       for (int c = 0; c < NU; ++c) {
         const R um = bu[(c * EPB + e) * KU + k];           // u- - u0

@@ -88,6 +88,25 @@ struct VCfg {
   static constexpr int W1 = w1(EPB);
   static constexpr int NCOLD = round_up(NC * EPB, 8);      // divergence columns
 
+  // ---- flux-volume kernel (gradients from HBM): no gradient operands or
+  // staging; element tiles sized so the pointwise phase fills the block
+  static constexpr int NT3 = TF32 ? 256 : 128;
+  static constexpr int A_FLUX = NAC * DIM * MP * KU;
+  static constexpr __host__ __device__ int nnode3(int epb) { return epb * NP + (KUR - NP) + 4; }
+  static constexpr __host__ __device__ size_t flux_bytes(int epb, int nperm) {
+    return (size_t)(A_FLUX + nnode3(epb) * FST + NS * epb * NP + epb * GEO) * RB + NFN * 4 +
+           epb * NF * 4 + NP * NF * 2 + (size_t)nperm * NFP + 64;
+  }
+  // the largest tile with at most one node per thread and two blocks per SM
+  static constexpr __host__ __device__ int pick_epb3() {
+    int best = 1;
+    for (int e = 1; e * NP <= NT3; ++e)
+      if (flux_bytes(e, 32) <= (size_t)BUDGET) best = e;
+    return best;
+  }
+  static constexpr int EPB3 = pick_epb3();
+  static constexpr int NCOL3 = round_up(NC * EPB3, 8);
+
   // ---- face kernel
   static constexpr int NT2 = 128;
   static constexpr int MINB2 = TF32 ? 4 : 3;
@@ -112,7 +131,8 @@ namespace {
 // allocation of the pointwise phase.
 template <class R, int DIM, int NS, bool MIX, bool VISC>
 __device__ __noinline__ void boundary_record(const DGArgs<R> a, const GasParams g, int bf, int m,
-                                             int nfp, const R* gq, R n0, R n1, R n2, R* dst) {
+                                             int nfp, const R* gq, int64_t gs, R n0, R n1, R n2,
+                                             R* dst) {
   constexpr int NC = DIM + 2 + NS, TW = trace_width(NC);
   const R n[3] = {n0, n1, n2};
   const int64_t bstride = (int64_t)a.nbf * nfp, bo = (int64_t)bf * nfp + m;
@@ -132,9 +152,9 @@ __device__ __noinline__ void boundary_record(const DGArgs<R> a, const GasParams 
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
-      for (int j = 0; j < DIM; ++j) gqv[c][j] = gq[c * DIM + j];
+      for (int j = 0; j < DIM; ++j) gqv[c][j] = gq[(c * DIM + j) * gs];
 #pragma unroll
-    for (int j = 0; j < DIM; ++j) gt[j] = gq[NC * DIM + j];
+    for (int j = 0; j < DIM; ++j) gt[j] = gq[(NC * DIM + j) * gs];
     R fv[NC][DIM];
     viscous_flux<R, DIM, NS, MIX>(sp, gqv, gt, fv);
 #pragma unroll
@@ -162,39 +182,6 @@ __device__ __noinline__ void boundary_record(const DGArgs<R> a, const GasParams 
   for (int c = 0; c < NC; ++c) a.bplus[c * bstride + bo] = qp[c];
 }
 
-// Interior state of a boundary face node: q- from HBM, the operator
-// temperature (mixtures) or the ideal gas's, and p, c, gamma.
-template <class R, int DIM, int NS, bool MIX>
-__device__ __forceinline__ void boundary_minus(const DGArgs<R>& a, const GasParams& g, int64_t EN,
-                                               int64_t gm, R* qm, NodeState<R, DIM, NS>& sm) {
-  constexpr int NC = DIM + 2 + NS;
-#pragma unroll
-  for (int c = 0; c < NC; ++c) qm[c] = a.q[c * EN + gm];
-  make_state<R, DIM, NS>(qm, MIX ? a.t_op[gm] : R(0), g, sm);
-}
-
-// The gradient pass's face value at a Mengaldo boundary face node:
-// (state_bc.cv, temperature_bc) into up[NC + 1] (boundary.py:732-793).
-template <class R, int DIM, int NS, bool MIX>
-__device__ __noinline__ void mengaldo_grad_value(const DGArgs<R> a, const GasParams g, int kind,
-                                                 int bf, int m, int nfp, int64_t EN, int64_t gm,
-                                                 R n0, R n1, R n2, R* up) {
-  constexpr int NC = DIM + 2 + NS;
-  const R n[3] = {n0, n1, n2};
-  R qm[NC];
-  NodeState<R, DIM, NS> sm;
-  boundary_minus<R, DIM, NS, MIX>(a, g, EN, gm, qm, sm);
-  R par[NC + 1];
-  const int64_t bstride = (int64_t)a.nbf * nfp, bo = (int64_t)bf * nfp + m;
-#pragma unroll
-  for (int c = 0; c <= NC; ++c) par[c] = bk_needs_bext(kind) ? a.bext[c * bstride + bo] : R(0);
-  R qbc[NC];
-  const R tbc = bc_state_cv<R, DIM, NS>(kind, g, qm, sm.t, sm.p, sm.c, sm.gamma, n, par, qbc);
-#pragma unroll
-  for (int c = 0; c < NC; ++c) up[c] = qbc[c];
-  up[NC] = tbc;
-}
-
 // The exterior record of a Mengaldo boundary face node (neighbour
 // convention) and its state_plus q into bplus.  The face kernel combines it
 // with the interior record as for an interior face: central(F_V) from the
@@ -204,7 +191,7 @@ __device__ __noinline__ void mengaldo_grad_value(const DGArgs<R> a, const GasPar
 template <class R, int DIM, int NS, bool MIX, bool VISC>
 __device__ __noinline__ void mengaldo_record(const DGArgs<R> a, const GasParams g, int kind,
                                              int bf, int m, int nfp, int64_t EN, int64_t gm,
-                                             const R* gq, R n0, R n1, R n2, R* dst) {
+                                             const R* gq, int64_t gs, R n0, R n1, R n2, R* dst) {
   constexpr int NC = DIM + 2 + NS, TW = trace_width(NC);
   const R n[3] = {n0, n1, n2};
   R qm[NC];
@@ -238,9 +225,9 @@ __device__ __noinline__ void mengaldo_record(const DGArgs<R> a, const GasParams 
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
-      for (int j = 0; j < DIM; ++j) gqv[c][j] = gq[c * DIM + j];
+      for (int j = 0; j < DIM; ++j) gqv[c][j] = gq[(c * DIM + j) * gs];
 #pragma unroll
-    for (int j = 0; j < DIM; ++j) gt[j] = gq[NC * DIM + j];
+    for (int j = 0; j < DIM; ++j) gt[j] = gq[(NC * DIM + j) * gs];
     R fvm[NC][DIM];
     viscous_flux<R, DIM, NS, MIX>(sm, gqv, gt, fvm);
     bc_gradients<R, DIM, NS>(kind, qm, qbc, n, gqv, gt);
@@ -268,6 +255,20 @@ __device__ __noinline__ void mengaldo_record(const DGArgs<R> a, const GasParams 
   for (int i = 0; i < TW; ++i) dst[i] = rec[i];
 #pragma unroll
   for (int c = 0; c < NC; ++c) a.bplus[c * bstride + bo] = qp[c];
+}
+
+// Ask L2 for the 128-byte lines of [p, p + bytes), the work spread over the
+// block's threads: the next tile's contiguous inputs are fetched while the
+// current tile computes (prefetch.global.L2 does not block and takes no
+// registers; a line already resident costs nothing).
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes, int part = -1,
+                                            int nparts = 0) {
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(p) & ~uintptr_t(127);
+  const uintptr_t a1 = reinterpret_cast<uintptr_t>(p) + bytes;
+  const uintptr_t start = part < 0 ? threadIdx.x : (uintptr_t)part;
+  const uintptr_t step = part < 0 ? blockDim.x : (uintptr_t)nparts;
+  for (uintptr_t a = a0 + start * 128; a < a1; a += step * 128)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
 }
 
 // 16-byte vector store / load of one record (TW values, 16-byte aligned)
@@ -480,6 +481,21 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT),
       }
       __syncthreads();
 
+      // the next tile's rows of q and the temperatures, its geometry and
+      // face pairing, into L2 while this tile computes
+      {
+        const int tn = tile + gridDim.x;
+        if (tn < ntiles) {
+          const int e1 = tn * EPB, n1 = imin(EPB, a.nowned - e1);
+          const size_t row = (size_t)n1 * NP * sizeof(R);
+          for (int c = 0; c < NC; ++c) prefetch_l2(a.q + c * EN + (int64_t)e1 * NP, row);
+          if (MIX) prefetch_l2(a.t_op + (int64_t)e1 * NP, row);
+          if (MIX && a.add_sources) prefetch_l2(a.t_src + (int64_t)e1 * NP, row);
+          prefetch_l2(a.rx + (int64_t)e1 * DIM * DIM, (size_t)n1 * DIM * DIM * sizeof(R));
+          prefetch_l2(a.conn + (int64_t)e1 * NF, (size_t)n1 * NF * 4);
+        }
+      }
+
       // contraction and metric combination into gn[node][c * DIM + j]
       for (int w = warp; w < (NCOL / 8) * MT; w += nwarps) {
         const int nt = w / MT, t = w % MT;
@@ -639,20 +655,6 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT),
 #pragma unroll
         for (int i = NC + 4; i < TW; ++i) rec[i] = R(0);
         store_rec<R, TW>(a.trace + (((int64_t)(e0 + e) * NF + f) * NFP + m) * TW, rec);
-        const int cn = conn_s[e * NF + f];
-        if (cn < 0) {
-          const int bf = -(cn + 1);
-          const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
-          const bool have = !bk_needs_bext(kind) || a.bext;
-          if (kind == BK_PRESCRIBED && have)
-            boundary_record<R, DIM, NS, MIX, VISC>(
-                a, g, bf, m, NFP, VISC ? gn + n * GST : nullptr, nf[0], nf[1],
-                DIM > 2 ? nf[DIM - 1] : R(0), a.btrace + ((int64_t)bf * NFP + m) * TW);
-          else if (bk_mengaldo(kind) && have)
-            mengaldo_record<R, DIM, NS, MIX, VISC>(
-                a, g, kind, bf, m, NFP, EN, gnd, VISC ? gn + n * GST : nullptr, nf[0], nf[1],
-                DIM > 2 ? nf[DIM - 1] : R(0), a.btrace + ((int64_t)bf * NFP + m) * TW);
-        }
       }
       if (k == 0) {
         // element-constant shift of the face terms: F0 . n_f, every face
@@ -670,6 +672,31 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT),
         }
       }
     }
+    // exterior records of the tile's boundary face nodes, in a loop of their
+    // own: out of line calls inside the pointwise loop would make the
+    // compiler spill that loop's registers around them for every node
+    for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
+      const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
+      const int cn = conn_s[e * NF + f];
+      if (cn >= 0) continue;
+      const int bf = -(cn + 1);
+      const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
+      if ((bk_needs_bext(kind) && !a.bext) || (kind != BK_PRESCRIBED && !bk_mengaldo(kind)))
+        continue;
+      const int k = fn_s[fm];
+      const int n = e * NP + k;
+      const R* nf = nrm_s + (e * NF + f) * DIM;
+      R* dst = a.btrace + ((int64_t)bf * NFP + m) * TW;
+      if (kind == BK_PRESCRIBED)
+        boundary_record<R, DIM, NS, MIX, VISC>(a, g, bf, m, NFP, VISC ? gn + n * GST : nullptr,
+                                               1, nf[0], nf[1], DIM > 2 ? nf[DIM - 1] : R(0),
+                                               dst);
+      else
+        mengaldo_record<R, DIM, NS, MIX, VISC>(a, g, kind, bf, m, NFP, EN,
+                                               (int64_t)(e0 + e) * NP + k,
+                                               VISC ? gn + n * GST : nullptr, 1, nf[0], nf[1],
+                                               DIM > 2 ? nf[DIM - 1] : R(0), dst);
+    }
     __syncthreads();
 
     // ---- volume divergence: rhs = -sum_r W_r (G_r - G0_r) (+ sources); one
@@ -686,6 +713,253 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT),
 #pragma unroll
         for (int v = 0; v < NACC; ++v) d[u][v] = R(0);
       // this lane's B column per n-tile: element row base and field offset
+      int cbase[NTG];
+#pragma unroll
+      for (int u = 0; u < NTG; ++u) {
+        const int col = (ngp * NTG + u) * 8 + gq;
+        const int c = col / EPB, e = col % EPB;
+        cbase[u] = (c < NC) ? (e * NP) * FST + c * DIM : -1;
+      }
+#pragma unroll
+      for (int r = 0; r < DIM; ++r) {
+        R g0[NTG];
+#pragma unroll
+        for (int u = 0; u < NTG; ++u) g0[u] = cbase[u] >= 0 ? gfl[cbase[u] + r] : R(0);
+        if constexpr (!V::TF32) {
+#pragma unroll
+          for (int ks = 0; ks < KUR / 4; ++ks) {
+            const double av = aw[(r * MP + t * 8 + gq) * KU + ks * 4 + tq];
+            const int kk = ks * 4 + tq;
+#pragma unroll
+            for (int u = 0; u < NTG; ++u) {
+              const double b = cbase[u] >= 0 ? gfl[cbase[u] + kk * FST + r] - g0[u] : 0.0;
+              dmma884(d[u], av, b);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int ks = 0; ks < KUR / 8; ++ks) {
+            uint32_t ah[4], alo[4];
+            load_a_tf32_ldsm(ah, aw + r * MP * KU, KU, t * 16, ks * 8, lane);
+            load_a_tf32_ldsm(alo, aw + AWN + r * MP * KU, KU, t * 16, ks * 8, lane);
+            const int k0 = ks * 8 + tq;
+#pragma unroll
+            for (int u = 0; u < NTG; ++u) {
+              float b0 = 0.f, b1 = 0.f;
+              if (cbase[u] >= 0) {
+                b0 = gfl[cbase[u] + k0 * FST + r] - g0[u];
+                b1 = gfl[cbase[u] + (k0 + 4) * FST + r] - g0[u];
+              }
+              mma_tf32x3(d[u], ah, alo, b0, b1);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < NTG; ++u)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int col = (ngp * NTG + u) * 8 + 2 * tq + h;
+          const int c = col / EPB, e = col % EPB;
+          if (c >= NC || e >= ne) continue;
+          R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
+#pragma unroll
+          for (int half = 0; half < NACC / 2; ++half) {
+            const int i = t * MROW + gq + 8 * half;
+            if (i >= NP) continue;
+            R v = -d[u][2 * half + h];
+            if (sources && c >= 2 + DIM) v += src_s[(c - 2 - DIM) * ENP + e * NP + i];
+            outp[i] = v;
+          }
+        }
+    }
+  }
+  if (bad) atomicOr(a.status, ST_NAN);
+}
+
+// Flux-volume kernel: the pointwise phase and the volume divergence of
+// k_volume with the gradients read from HBM (written by k_grad), for the
+// three-kernel pass gradient -> flux-volume -> face.  Without the gradient
+// operands and staging its tiles fill the block: 12 order-3 tetrahedra (240
+// nodes) per 256 threads on the float32 path.
+template <class R, int DIM, int ORDER, int NS, bool MIX, bool VISC>
+__global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT3), 2)
+    k_flux_volume(DGArgs<R> a, GasParams g) {
+  using V = VCfg<R, DIM, ORDER, NS, MIX>;
+  using S = Simplex<DIM, ORDER>;
+  constexpr int NP = V::NP, NF = V::NF, NFP = V::NFP, NFN = V::NFN, NC = V::NC;
+  constexpr int EPB = V::EPB3, MP = V::MP, MT = V::MT, MROW = V::MROW;
+  constexpr int KU = V::KU, KUR = V::KUR, NCOLD = V::NCOL3, NNODE = V::nnode3(V::EPB3);
+  constexpr int FST = V::FST, TW = V::TW;
+  constexpr int AWN = DIM * MP * KU;
+  constexpr int ENP = EPB * NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* aw = reinterpret_cast<R*>(smem_raw);                  // [NAC][DIM][MP][KU]
+  R* gfl = aw + V::A_FLUX;                                 // [NNODE][FST]
+  R* src_s = gfl + NNODE * FST;                            // [NS][ENP]
+  R* rx_s = src_s + NS * ENP;                              // [EPB][DIM][DIM]
+  R* nrm_s = rx_s + EPB * DIM * DIM;                       // [EPB][NF][DIM]
+  R* fs_s = nrm_s + EPB * NF * DIM;                        // [EPB][NF]
+  int* fn_s = reinterpret_cast<int*>(fs_s + EPB * NF);     // [NFN]
+  int32_t* conn_s = fn_s + NFN;                            // [EPB][NF]
+  int16_t* slot_s = reinterpret_cast<int16_t*>(conn_s + EPB * NF);   // [NP][NF]
+
+  const int E = a.nelem;
+  const int64_t EN = (int64_t)E * NP;
+  const bool sources = MIX && a.add_sources;
+  for (int i = threadIdx.x; i < AWN; i += blockDim.x) {
+    const int r = i / (MP * KU), row = (i / KU) % MP, k = i % KU;
+    put_a<R>(aw, AWN, i, (row < NP && k < NP) ? c_ref64[S::OFF_W + (r * NP + row) * NP + k] : 0.0);
+  }
+  for (int i = threadIdx.x; i < NNODE * FST + NS * ENP; i += blockDim.x) gfl[i] = R(0);
+  for (int i = threadIdx.x; i < NFN; i += blockDim.x) fn_s[i] = c_face_nodes<DIM, ORDER>(i);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NP * NF; ++i) slot_s[i] = -1;
+    for (int fm = 0; fm < NFN; ++fm) {
+      const int k = c_face_nodes<DIM, ORDER>(fm);
+      for (int sl = 0; sl < NF; ++sl)
+        if (slot_s[k * NF + sl] < 0) {
+          slot_s[k * NF + sl] = (int16_t)fm;
+          break;
+        }
+    }
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int nwarps = blockDim.x >> 5;
+  constexpr int NACC = V::TF32 ? 4 : 2;
+  const int ntiles = (a.nowned + EPB - 1) / EPB;
+  bool bad = false;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int e0 = tile * EPB;
+    const int ne = imin(EPB, a.nowned - e0);
+    __syncthreads();
+    stage_conn<NF>(a.conn, e0, ne, conn_s);
+    load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
+    __syncthreads();
+
+    for (int n = threadIdx.x; n < ne * NP; n += blockDim.x) {
+      const int e = n / NP, k = n % NP;
+      const int64_t gnd = (int64_t)(e0 + e) * NP + k;
+      R qq[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) qq[c] = a.q[c * EN + gnd];
+      NodeState<R, DIM, NS> st;
+      make_state<R, DIM, NS>(qq, MIX ? a.t_op[gnd] : R(0), g, st);
+      R fl[NC][DIM];
+      inviscid_flux<R, DIM, NS>(st, fl);
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) fl[c][j] = -fl[c][j];
+      if constexpr (VISC) {
+        R gqv[NC][DIM], gt[DIM];
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+          for (int j = 0; j < DIM; ++j) gqv[c][j] = a.grad[((int64_t)c * DIM + j) * EN + gnd];
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) gt[j] = a.grad[((int64_t)NC * DIM + j) * EN + gnd];
+        R fv[NC][DIM];
+        viscous_flux<R, DIM, NS, MIX>(st, gqv, gt, fv);
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+          for (int j = 0; j < DIM; ++j) fl[c][j] = fv[c][j] + fl[c][j];
+      }
+      bad |= !(st.p == st.p) || !(st.c == st.c);
+      const R* rxe = rx_s + e * DIM * DIM;
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) {
+          R acc = R(0);
+#pragma unroll
+          for (int j = 0; j < DIM; ++j) acc += rxe[r * DIM + j] * fl[c][j];
+          gfl[n * FST + c * DIM + r] = acc;
+        }
+      if constexpr (MIX && NS > 0) {
+        if (sources) {
+          R om[NS];
+          production_rates<R, NS>(st.rho, a.t_src[gnd], st.y, (R)g.zero_level, om);
+#pragma unroll
+          for (int sp = 0; sp < NS; ++sp) src_s[sp * ENP + n] = mech<R>().mw[sp] * om[sp];
+        }
+      }
+      R v2 = R(0);
+#pragma unroll
+      for (int j = 0; j < DIM; ++j) v2 += st.v[j] * st.v[j];
+      const R lam = sqrt(v2) + st.c;
+#pragma unroll 1
+      for (int sl = 0; sl < NF; ++sl) {
+        const int fm = slot_s[k * NF + sl];
+        if (fm < 0) break;
+        const int f = fm / NFP, m = fm % NFP;
+        const R* nf = nrm_s + (e * NF + f) * DIM;
+        R rec[TW];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          R acc = R(0);
+#pragma unroll
+          for (int j = 0; j < DIM; ++j) acc += fl[c][j] * nf[j];
+          rec[c] = acc;
+        }
+        rec[NC] = lam;
+        rec[NC + 1] = st.p;
+        rec[NC + 2] = st.c;
+        rec[NC + 3] = st.gamma;
+#pragma unroll
+        for (int i = NC + 4; i < TW; ++i) rec[i] = R(0);
+        store_rec<R, TW>(a.trace + (((int64_t)(e0 + e) * NF + f) * NFP + m) * TW, rec);
+      }
+      if (k == 0) {
+        R* s0e = a.s0 + (int64_t)(e0 + e) * NF * NC;
+#pragma unroll 1
+        for (int f = 0; f < NF; ++f) {
+          const R* nf = nrm_s + (e * NF + f) * DIM;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            R acc = R(0);
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) acc += fl[c][j] * nf[j];
+            s0e[f * NC + c] = acc;
+          }
+        }
+      }
+    }
+    // exterior records of the tile's boundary face nodes (own loop: see k_volume)
+    for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
+      const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
+      const int cn = conn_s[e * NF + f];
+      if (cn >= 0) continue;
+      const int bf = -(cn + 1);
+      const int kind = (bf < a.nbf) ? a.bkind[bf] : -1;
+      if ((bk_needs_bext(kind) && !a.bext) || (kind != BK_PRESCRIBED && !bk_mengaldo(kind)))
+        continue;
+      const int64_t gnd = (int64_t)(e0 + e) * NP + fn_s[fm];
+      const R* nf = nrm_s + (e * NF + f) * DIM;
+      R* dst = a.btrace + ((int64_t)bf * NFP + m) * TW;
+      if (kind == BK_PRESCRIBED)
+        boundary_record<R, DIM, NS, MIX, VISC>(a, g, bf, m, NFP, VISC ? a.grad + gnd : nullptr,
+                                               EN, nf[0], nf[1], DIM > 2 ? nf[DIM - 1] : R(0),
+                                               dst);
+      else
+        mengaldo_record<R, DIM, NS, MIX, VISC>(a, g, kind, bf, m, NFP, EN, gnd,
+                                               VISC ? a.grad + gnd : nullptr, EN, nf[0], nf[1],
+                                               DIM > 2 ? nf[DIM - 1] : R(0), dst);
+    }
+    __syncthreads();
+
+    // volume divergence (as k_volume)
+    constexpr int NNT = NCOLD / 8;
+    constexpr int NTG = (NNT % 3 == 0) ? 3 : ((NNT % 2 == 0) ? 2 : 1);
+    for (int w = warp; w < (NNT / NTG) * MT; w += nwarps) {
+      const int ngp = w / MT, t = w % MT;
+      R d[NTG][NACC];
+#pragma unroll
+      for (int u = 0; u < NTG; ++u)
+#pragma unroll
+        for (int v = 0; v < NACC; ++v) d[u][v] = R(0);
       int cbase[NTG];
 #pragma unroll
       for (int u = 0; u < NTG; ++u) {
@@ -834,6 +1108,22 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT2),
     stage_conn<NF>(a.conn, e0, ne, conn_s);
     load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
     __syncthreads();
+    // the next tile's own records, shifts, q and rhs rows into L2
+    {
+      const int tn = tile + gridDim.x;
+      if (tn < ntiles) {
+        const int e1 = tn * EPB, n1 = imin(EPB, a.nowned - e1);
+        prefetch_l2(a.trace + (int64_t)e1 * NFN * TW, (size_t)n1 * NFN * TW * sizeof(R));
+        prefetch_l2(a.s0 + (int64_t)e1 * NF * NC, (size_t)n1 * NF * NC * sizeof(R));
+        const size_t row = (size_t)n1 * NP * sizeof(R);
+        for (int c = 0; c < NC; ++c) {
+          prefetch_l2(a.q + c * EN + (int64_t)e1 * NP, row);
+          prefetch_l2(a.out + c * EN + (int64_t)e1 * NP, row);
+        }
+        prefetch_l2(a.rx + (int64_t)e1 * DIM * DIM, (size_t)n1 * DIM * DIM * sizeof(R));
+        prefetch_l2(a.conn + (int64_t)e1 * NF, (size_t)n1 * NF * 4);
+      }
+    }
 
     for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
       const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
@@ -892,23 +1182,44 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT2),
                                             EPB * KF);
         continue;
       }
+      // every load of the face node issued before any use (read-only path)
       R rm[TW], rp[TW];
       load_record<R, TW>(recm, rm);
       load_record<R, TW>(recp, rp);
-      R qm[NC], qp[NC];
+      R qm[NC], qp[NC], sh[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        qm[c] = a.q[c * EN + gm];
-        qp[c] = qp_g[c * qstride];
+        qm[c] = __ldg(a.q + c * EN + gm);
+        qp[c] = __ldg(qp_g + c * qstride);
+        sh[c] = __ldg(s0 + c);
       }
       const R lam = (a.flux_kind == FLUX_RUSANOV) ? fmax(rm[NC], rp[NC]) : R(0);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         const R out = (rm[c] - rp[c]) / R(2) - lam * (qm[c] - qp[c]) / R(2);
-        bcol[c * EPB * KF] = fsc * (out - s0[c]);
+        bcol[c * EPB * KF] = fsc * (out - sh[c]);
       }
     }
     __syncthreads();
+    // the next tile's neighbour face records and neighbour q rows into L2
+    // while this tile's lift runs (its face pairing is read from HBM here)
+    {
+      const int tn = tile + gridDim.x;
+      if (tn < ntiles) {
+        const int e1 = tn * EPB, n1 = imin(EPB, a.nowned - e1);
+        for (int it = threadIdx.x; it < n1 * NF; it += blockDim.x) {
+          const int cn = __ldg(a.conn + (int64_t)e1 * NF + it);
+          if (cn < 0) continue;
+          const int en = cn >> 8, pr = cn & 255;
+          if (en >= E || pr >= a.nperm) continue;
+          const int fo = fslot_s[pr * NFP] / NFP;
+          prefetch_l2(a.trace + ((int64_t)en * NF + fo) * NFP * TW, (size_t)NFP * TW * sizeof(R),
+                      0, 1);
+          for (int c = 0; c < NC; ++c)
+            prefetch_l2(a.q + c * EN + (int64_t)en * NP, (size_t)NP * sizeof(R), 0, 1);
+        }
+      }
+    }
 
     // rhs += LIFT S on the tensor cores; one m-tile and NTG n-tiles per item
     constexpr int NNT = NCOL / 8;

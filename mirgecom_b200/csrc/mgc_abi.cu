@@ -1,6 +1,7 @@
 // extern "C" entry points of libmgc_b200 (declared in include/mgc_b200.h).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
 #include <vector>
 
@@ -100,6 +101,9 @@ int ready(const mgc_mesh_t* m, const mgc_gas_t* g) {
   return MGC_OK;
 }
 
+// gradient-pass kernel choice (mgc_set_gradient_kernel), process-wide
+std::atomic<int> g_grad_kernel{MGC_GRAD_AUTO};
+
 template <class R>
 DGArgs<R> make_args(const mgc_mesh_t* m, const R* q, const R* t_op, const R* t_src,
                     const R* grad, R* out, const R* bext, int flux_kind, int add_sources,
@@ -126,6 +130,7 @@ DGArgs<R> make_args(const mgc_mesh_t* m, const R* q, const R* t_op, const R* t_s
   a.bext = bext;
   a.status = status;
   a.add_sources = add_sources;
+  a.grad_kernel = g_grad_kernel.load(std::memory_order_relaxed) == MGC_GRAD_MMA_SYNC ? 1 : 0;
   return a;
 }
 
@@ -253,7 +258,9 @@ int operator_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const 
                   const R* t_op, const R* t_src, const R* bext, int flux_kind, int add_sources,
                   R* rhs, R* grad_out, void* workspace, size_t workspace_bytes, int32_t* status,
                   void* stream, void* mid_event, int phases) {
-  if (phases < 1 || phases > 3) return MGC_E_INVALID;
+  if (phases < 1 || phases > 15 || (phases & 3) == 0) return MGC_E_INVALID;
+  if ((phases & 8) && !(phases & 4)) return MGC_E_INVALID;
+  if ((phases & 4) && (phases & 1) && visc && !grad_out) return MGC_E_INVALID;
   if (!mesh_ok(mesh) || !gas_ok(gas) || !q || !rhs || !status || !workspace)
     return MGC_E_INVALID;
   if (flux_kind < 0 || flux_kind > 2) return MGC_E_INVALID;
@@ -281,13 +288,21 @@ int operator_impl(int visc, const mgc_mesh_t* mesh, const mgc_gas_t* gas, const 
   a.grad_out = grad_out;
   a.mid_event = mid_event;
   a.nowned = mesh->nowned > 0 ? mesh->nowned : mesh->nelem;
-  const int op = (phases == 3) ? 5 : (phases == 1 ? 7 : 9);
-  return dispatch(op + (visc ? 1 : 0), mesh, gas, a, (cudaStream_t)stream);
+  a.phases = phases;
+  return dispatch(visc ? 6 : 5, mesh, gas, a, (cudaStream_t)stream);
 }
 
 }  // namespace
 
 extern "C" {
+
+int mgc_set_gradient_kernel(int kind) {
+  if (kind != MGC_GRAD_AUTO && kind != MGC_GRAD_MMA_SYNC) return MGC_E_INVALID;
+  g_grad_kernel.store(kind);
+  return MGC_OK;
+}
+
+int mgc_get_gradient_kernel(void) { return g_grad_kernel.load(); }
 
 size_t mgc_operator_workspace_bytes(const mgc_mesh_t* mesh, const mgc_gas_t* gas,
                                     int single_precision) {

@@ -123,6 +123,7 @@ enum StatusBits {
   ST_BAD_INDEX = 2,
   ST_NEWTON_MISS = 4,
   ST_NONPOSITIVE = 8,
+  ST_WAIT_TIMEOUT = 16,   // a bounded wait inside a pipelined kernel ran out
 };
 
 template <class R> __device__ __forceinline__ R rsqrt_(R x);

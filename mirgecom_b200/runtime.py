@@ -270,16 +270,23 @@ def _operator_temperature(state):
 #   "volume_face"  two kernels: volume (gradients kept on chip, pointwise
 #                  fluxes, face-node records, volume divergence) and face
 #                  (numerical fluxes from the records, lift) -- mgc_operator*
+#   "gradient_volume_face"  three kernels through mgc_operator* (phases bit
+#                  2): gradients into HBM, flux-volume (pointwise fluxes,
+#                  records, volume divergence), face
 #   "split"        three kernels: gradients, per-node flux records, surface
 #                  and lift -- mgc_ns_grad* + mgc_rhs_split*
 #   "fused"        two kernels: gradients, fused divergence -- mgc_ns_grad* +
 #                  mgc_ns_rhs* (mgc_euler_rhs* for the Euler operator)
 # Tensor-product hexahedra always take "split".
-RHS_PATH = "volume_face"
+RHS_PATH = "gradient_volume_face"
 
 
 def _path(dcoll):
     return "split" if dcoll.refel.kind == "hypercube" else RHS_PATH
+
+
+def _operator_path(path):
+    return path in ("volume_face", "gradient_volume_face")
 
 
 def _split_workspace(dd, gs, f32):
@@ -342,7 +349,7 @@ def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
     lib = _lib.load()
     dd = device_discretization(dcoll, q.device)
     gs = _gas_struct(gas_model, state.cv.nspecies, q.device)
-    if _path(dcoll) != "volume_face":
+    if not _operator_path(_path(dcoll)):
         # the inviscid slip wall needs only its state_plus: prescribe it
         from mirgecom_b200.boundary import AdiabaticSlipBoundary, _SlipStatePlus
         boundaries = {t: (_SlipStatePlus() if isinstance(b, AdiabaticSlipBoundary) else b)
@@ -356,8 +363,9 @@ def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
     f32 = q.dtype == torch.float32
     path = _path(dcoll)
     with torch.cuda.device(q.device):
-        if path == "volume_face":
-            _run_operator(False, dd, gs, q, t_op, None, bext, flux_kind, False, rhs, None)
+        if _operator_path(path):
+            _run_operator(False, dd, gs, q, t_op, None, bext, flux_kind, False, rhs, None,
+                          phases=3 | (4 if path == "gradient_volume_face" else 0))
         elif path == "split":
             ws = _split_workspace(dd, gs, f32)
             fsplit = lib.mgc_rhs_split_f32 if f32 else lib.mgc_rhs_split
@@ -374,11 +382,22 @@ def euler_rhs(dcoll, state, gas_model, boundaries, time, flux_kind):
     return rhs
 
 
+def set_gradient_kernel(kind):
+    """Select the gradient-pass kernel process-wide: "auto" (the tcgen05
+    pipelined kernel where it applies, else mma.sync) or "mma_sync"."""
+    code = {"auto": 0, "mma_sync": 1}[kind]
+    _lib.check(_lib.load().mgc_set_gradient_kernel(code), "mgc_set_gradient_kernel")
+
+
+def gradient_kernel():
+    return {0: "auto", 1: "mma_sync"}[_lib.load().mgc_get_gradient_kernel()]
+
+
 def _check_boundary_path(dcoll, boundaries):
     """The Mengaldo boundaries are evaluated by the volume/face path only."""
     from mirgecom_b200.boundary import MengaldoBoundaryCondition
     bad = [t for t, b in boundaries.items() if isinstance(b, MengaldoBoundaryCondition)]
-    if bad and _path(dcoll) != "volume_face":
+    if bad and not _operator_path(_path(dcoll)):
         raise NotImplementedError(
             f"boundaries {bad}: the Mengaldo treatment runs on the volume/face path of "
             "simplicial meshes only")
@@ -391,9 +410,11 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
     Gradients [Nc+1, dim, E, Np] are returned when *want_gradients* (they are
     only written to HBM then, on the volume/face path).  *events*: on the
     volume/face path 3 CUDA events (before the volume kernel, between the
-    two kernels, after the face kernel); on the other paths 3 or 4 (before
-    the gradient pass, between the passes, [between the node-flux and surface
-    kernels,] after the divergence).
+    two kernels, after the face kernel); on the gradient/volume/face path 4
+    (before the gradient kernel, before the flux-volume kernel, before the
+    face kernel, after it); on the other paths 3 or 4 (before the gradient
+    pass, between the passes, [between the node-flux and surface kernels,]
+    after the divergence).
 
     Mesh partitions (*dcoll* a :class:`~mirgecom_b200.partition.
     PartitionedDiscretization`, the state's ghost rows already exchanged):
@@ -423,19 +444,36 @@ def ns_rhs(dcoll, state, gas_model, boundaries, time, flux_kind, *,
     f32 = q.dtype == torch.float32
     path = _path(dcoll)
     gshape = (nc + 1, dcoll.dim) + tuple(q.shape[1:])
-    if path == "volume_face":
-        grad = torch.empty(gshape, dtype=q.dtype, device=q.device) if want_gradients else None
+    if _operator_path(path):
+        three = path == "gradient_volume_face"
+        if three:
+            grad = dd.workspace("grad", gshape, q.dtype)
+        else:
+            grad = torch.empty(gshape, dtype=q.dtype, device=q.device) if want_gradients else None
+        # three kernels: the gradient entry point (its own launch, timed by
+        # events[0..1]), then the operator with the gradients given (bit 8)
+        extra = 4 | 8 if three else 0
+        ops_events = events[1:] if (events and three) else events
         with torch.cuda.device(q.device):
+            if three and (phases & 1):
+                if events:
+                    events[0].record()
+                fgrad = lib.mgc_ns_grad_f32 if f32 else lib.mgc_ns_grad
+                _lib.check(fgrad(
+                    C.byref(dd.mesh), C.byref(gs), _lib.ptr(q), _lib.ptr(t_op), _lib.ptr(bext),
+                    _lib.ptr(grad), _lib.ptr(dd.status), stream), "mgc_ns_grad")
             if halo is None:
                 _run_operator(True, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs, grad,
-                              events=events, phases=phases)
+                              events=ops_events, phases=phases | (extra if phases & 1 else 0))
             else:
                 _run_operator(True, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs, grad,
-                              phases=1)
+                              phases=1 | extra)
                 halo.exchange_records(face_records(dd, gs, f32, nc))
                 _run_operator(True, dd, gs, q, t_op, t_src, bext, flux_kind, add_src, rhs, None,
                               phases=2)
-        return rhs, grad
+        if three and want_gradients:
+            grad = grad.clone()
+        return rhs, (grad if want_gradients else None)
     grad = dd.workspace("grad", gshape, q.dtype)
     fgrad = lib.mgc_ns_grad_f32 if f32 else lib.mgc_ns_grad
     frhs = lib.mgc_ns_rhs_f32 if f32 else lib.mgc_ns_rhs
@@ -495,14 +533,10 @@ def rk4_stage(q0, k, acc, qout, stage, dt, qout_lo=None):
 
 
 def ns_gradients(dcoll, state, gas_model, boundaries, time):
-    """The BR1 gradients [Nc+1, dim, E, Np] (a workspace tensor): the gradient
-    kernel mgc_ns_grad*, or, where a Mengaldo boundary needs the volume/face
-    path's boundary treatment, that path's gradient output."""
-    from mirgecom_b200.boundary import MengaldoBoundaryCondition
-    if any(isinstance(b, MengaldoBoundaryCondition) for b in boundaries.values()):
-        _check_boundary_path(dcoll, boundaries)
-        _, grad = ns_rhs(dcoll, state, gas_model, boundaries, time, 0, want_gradients=True)
-        return grad
+    """The BR1 gradients [Nc+1, dim, E, Np] (a workspace tensor) from the
+    gradient kernel mgc_ns_grad* (its Mengaldo boundary states on simplices
+    included)."""
+    _check_boundary_path(dcoll, boundaries)
     q = state.cv.q
     _lib.require_cuda(q)
     q = q.contiguous()

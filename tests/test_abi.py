@@ -49,7 +49,19 @@ def test_invalid_arguments_rejected_without_gpu():
 _QUERIES = {"mgc_version", "mgc_supports", "mgc_supports_hex", "mgc_mlp_nparams",
             "mgc_rhs_split_workspace_bytes", "mgc_mlp_train_workspace_bytes",
             "mgc_ns_operator_noalloc_capacity", "mgc_fp64_probe_flops",
-            "mgc_operator_workspace_bytes"}
+            "mgc_operator_workspace_bytes", "mgc_set_gradient_kernel",
+            "mgc_get_gradient_kernel"}
+
+
+def test_gradient_kernel_option_without_gpu():
+    lib = _lib.load()
+    assert lib.mgc_get_gradient_kernel() == 0
+    assert lib.mgc_set_gradient_kernel(7) == -1
+    assert lib.mgc_set_gradient_kernel(-1) == -1
+    assert lib.mgc_get_gradient_kernel() == 0
+    assert lib.mgc_set_gradient_kernel(1) == 0
+    assert lib.mgc_get_gradient_kernel() == 1
+    assert lib.mgc_set_gradient_kernel(0) == 0
 
 
 def _null_call_script():

@@ -253,13 +253,15 @@ def test_rhs_paths_agree(cuda, case):
         kw, flux = {}, inviscid_facial_flux_hll
         floor = inviscid_flux_floor(q, 2, 0.2)
     outs = {}
-    for path in ("volume_face", "split", "fused"):
+    default = runtime.RHS_PATH
+    for path in ("volume_face", "gradient_volume_face", "split", "fused"):
         runtime.RHS_PATH = path
         try:
             outs[path] = ns_operator(d, gas, st, bnds, inviscid_numerical_flux_func=flux,
                                      **kw).q.cpu().numpy()
         finally:
-            runtime.RHS_PATH = "volume_face"
+            runtime.RHS_PATH = default
     assert_fields_close(outs["split"], outs["fused"], TOL, floor=floor)
     assert_fields_close(outs["volume_face"], outs["fused"], TOL, floor=floor)
+    assert_fields_close(outs["gradient_volume_face"], outs["fused"], TOL, floor=floor)
     _status_ok(d)
