@@ -261,13 +261,10 @@ __device__ __noinline__ void mengaldo_record(const DGArgs<R> a, const GasParams 
 // block's threads: the next tile's contiguous inputs are fetched while the
 // current tile computes (prefetch.global.L2 does not block and takes no
 // registers; a line already resident costs nothing).
-__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes, int part = -1,
-                                            int nparts = 0) {
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
   const uintptr_t a0 = reinterpret_cast<uintptr_t>(p) & ~uintptr_t(127);
   const uintptr_t a1 = reinterpret_cast<uintptr_t>(p) + bytes;
-  const uintptr_t start = part < 0 ? threadIdx.x : (uintptr_t)part;
-  const uintptr_t step = part < 0 ? blockDim.x : (uintptr_t)nparts;
-  for (uintptr_t a = a0 + start * 128; a < a1; a += step * 128)
+  for (uintptr_t a = a0 + (uintptr_t)threadIdx.x * 128; a < a1; a += (uintptr_t)blockDim.x * 128)
     asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
 }
 
@@ -1108,22 +1105,6 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT2),
     stage_conn<NF>(a.conn, e0, ne, conn_s);
     load_geometry<R, DIM, ORDER>(a.rx, e0, ne, rx_s, nrm_s, fs_s);
     __syncthreads();
-    // the next tile's own records, shifts, q and rhs rows into L2
-    {
-      const int tn = tile + gridDim.x;
-      if (tn < ntiles) {
-        const int e1 = tn * EPB, n1 = imin(EPB, a.nowned - e1);
-        prefetch_l2(a.trace + (int64_t)e1 * NFN * TW, (size_t)n1 * NFN * TW * sizeof(R));
-        prefetch_l2(a.s0 + (int64_t)e1 * NF * NC, (size_t)n1 * NF * NC * sizeof(R));
-        const size_t row = (size_t)n1 * NP * sizeof(R);
-        for (int c = 0; c < NC; ++c) {
-          prefetch_l2(a.q + c * EN + (int64_t)e1 * NP, row);
-          prefetch_l2(a.out + c * EN + (int64_t)e1 * NP, row);
-        }
-        prefetch_l2(a.rx + (int64_t)e1 * DIM * DIM, (size_t)n1 * DIM * DIM * sizeof(R));
-        prefetch_l2(a.conn + (int64_t)e1 * NF, (size_t)n1 * NF * 4);
-      }
-    }
 
     for (int fnode = threadIdx.x; fnode < ne * NFN; fnode += blockDim.x) {
       const int e = fnode / NFN, fm = fnode % NFN, f = fm / NFP, m = fm % NFP;
@@ -1182,16 +1163,15 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT2),
                                             EPB * KF);
         continue;
       }
-      // every load of the face node issued before any use (read-only path)
       R rm[TW], rp[TW];
       load_record<R, TW>(recm, rm);
       load_record<R, TW>(recp, rp);
       R qm[NC], qp[NC], sh[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        qm[c] = __ldg(a.q + c * EN + gm);
-        qp[c] = __ldg(qp_g + c * qstride);
-        sh[c] = __ldg(s0 + c);
+        qm[c] = a.q[c * EN + gm];
+        qp[c] = qp_g[c * qstride];
+        sh[c] = s0[c];
       }
       const R lam = (a.flux_kind == FLUX_RUSANOV) ? fmax(rm[NC], rp[NC]) : R(0);
 #pragma unroll
@@ -1201,25 +1181,6 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT2),
       }
     }
     __syncthreads();
-    // the next tile's neighbour face records and neighbour q rows into L2
-    // while this tile's lift runs (its face pairing is read from HBM here)
-    {
-      const int tn = tile + gridDim.x;
-      if (tn < ntiles) {
-        const int e1 = tn * EPB, n1 = imin(EPB, a.nowned - e1);
-        for (int it = threadIdx.x; it < n1 * NF; it += blockDim.x) {
-          const int cn = __ldg(a.conn + (int64_t)e1 * NF + it);
-          if (cn < 0) continue;
-          const int en = cn >> 8, pr = cn & 255;
-          if (en >= E || pr >= a.nperm) continue;
-          const int fo = fslot_s[pr * NFP] / NFP;
-          prefetch_l2(a.trace + ((int64_t)en * NF + fo) * NFP * TW, (size_t)NFP * TW * sizeof(R),
-                      0, 1);
-          for (int c = 0; c < NC; ++c)
-            prefetch_l2(a.q + c * EN + (int64_t)en * NP, (size_t)NP * sizeof(R), 0, 1);
-        }
-      }
-    }
 
     // rhs += LIFT S on the tensor cores; one m-tile and NTG n-tiles per item
     constexpr int NNT = NCOL / 8;
