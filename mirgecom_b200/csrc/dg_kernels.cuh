@@ -227,6 +227,7 @@ __device__ __forceinline__ void mma_tf32x3(float (&d)[4], const uint32_t (&ahi)[
 // B operand split once into tf32 hi/lo words (shared by several A operands)
 struct SplitB {
   uint32_t h0, h1, l0, l1;
+  SplitB() = default;
   __device__ __forceinline__ SplitB(float b0, float b1) {
     h0 = to_tf32(b0);
     h1 = to_tf32(b1);

@@ -947,9 +947,77 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT3), 2)
     }
     __syncthreads();
 
-    // volume divergence (as k_volume)
+    // volume divergence.  float32: one item per group of NTG column tiles
+    // and every m-tile, so each shifted flux value is read and split into
+    // its tf32 hi/lo words once
     constexpr int NNT = NCOLD / 8;
     constexpr int NTG = (NNT % 3 == 0) ? 3 : ((NNT % 2 == 0) ? 2 : 1);
+    if constexpr (V::TF32) {
+      for (int w = warp; w < NNT / NTG; w += nwarps) {
+        const int ngp = w;
+        float d[MT][NTG][NACC];
+#pragma unroll
+        for (int t = 0; t < MT; ++t)
+#pragma unroll
+          for (int u = 0; u < NTG; ++u)
+#pragma unroll
+            for (int v = 0; v < NACC; ++v) d[t][u][v] = 0.f;
+        int cbase[NTG];
+#pragma unroll
+        for (int u = 0; u < NTG; ++u) {
+          const int col = (ngp * NTG + u) * 8 + gq;
+          const int c = col / EPB, e = col % EPB;
+          cbase[u] = (c < NC) ? (e * NP) * FST + c * DIM : -1;
+        }
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) {
+          float g0[NTG];
+#pragma unroll
+          for (int u = 0; u < NTG; ++u) g0[u] = cbase[u] >= 0 ? gfl[cbase[u] + r] : 0.f;
+#pragma unroll
+          for (int ks = 0; ks < KUR / 8; ++ks) {
+            const int k0 = ks * 8 + tq;
+            SplitB bs[NTG] = {};
+#pragma unroll
+            for (int u = 0; u < NTG; ++u) {
+              float b0 = 0.f, b1 = 0.f;
+              if (cbase[u] >= 0) {
+                b0 = gfl[cbase[u] + k0 * FST + r] - g0[u];
+                b1 = gfl[cbase[u] + (k0 + 4) * FST + r] - g0[u];
+              }
+              bs[u] = SplitB(b0, b1);
+            }
+#pragma unroll
+            for (int t = 0; t < MT; ++t) {
+              uint32_t ah[4], alo[4];
+              load_a_tf32_ldsm(ah, aw + r * MP * KU, KU, t * 16, ks * 8, lane);
+              load_a_tf32_ldsm(alo, aw + AWN + r * MP * KU, KU, t * 16, ks * 8, lane);
+#pragma unroll
+              for (int u = 0; u < NTG; ++u) mma_tf32x3(d[t][u], ah, alo, bs[u]);
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < NTG; ++u)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int col = (ngp * NTG + u) * 8 + 2 * tq + h;
+            const int c = col / EPB, e = col % EPB;
+            if (c >= NC || e >= ne) continue;
+            R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
+#pragma unroll
+            for (int t = 0; t < MT; ++t)
+#pragma unroll
+              for (int half = 0; half < NACC / 2; ++half) {
+                const int i = t * MROW + gq + 8 * half;
+                if (i >= NP) continue;
+                R v = -d[t][u][2 * half + h];
+                if (sources && c >= 2 + DIM) v += src_s[(c - 2 - DIM) * ENP + e * NP + i];
+                outp[i] = v;
+              }
+          }
+      }
+    } else
     for (int w = warp; w < (NNT / NTG) * MT; w += nwarps) {
       const int ngp = w / MT, t = w % MT;
       R d[NTG][NACC];
