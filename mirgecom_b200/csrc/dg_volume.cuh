@@ -108,12 +108,15 @@ struct VCfg {
   static constexpr int NCOL3 = round_up(NC * EPB3, 8);
 
   // ---- face kernel
+  // float32: 8-element tiles in six resident blocks per SM (the face pass is
+  // bound by its gathers' latency: 8.7 ms against 9.8 ms for four blocks of
+  // 16 elements at 80^3)
   static constexpr int NT2 = 128;
-  static constexpr int MINB2 = TF32 ? 4 : 3;
+  static constexpr int MINB2 = TF32 ? 6 : 3;
   static constexpr int KFR = round_up(NFN, KSTEP);
   static constexpr int KF = Tile<R>::stride(KFR);
   static constexpr int A_FACE = NAC * MP * KF;
-  static constexpr int EPB2 = TF32 ? 16 : 8;
+  static constexpr int EPB2 = 8;
   static constexpr int NCOL2 = round_up(NC * EPB2, 8);
   static size_t face_bytes(int nperm) {
     return (size_t)(A_FACE + NCOL2 * KF + EPB2 * GEO) * RB + NFN * 4 + EPB2 * NF * 4 +
