@@ -400,7 +400,7 @@ def _time_form(dcoll, gas, q, tseed, steps, warmup, flush, stream):
     import torch
 
     from mirgecom_b200 import runtime
-    path = runtime._path(dcoll)
+    path = runtime._path(dcoll, gas)
     vf = path == "volume_face"
     three = path == "gradient_volume_face"
     nev = 4 if vf else 5
@@ -856,12 +856,16 @@ def _run_ours(args):
         dist.barrier()
     status = runtime.read_status(dcoll, dev)
     eor = None
-    if args.end_of_run > 0 and world == 1 and not args.profile:
+    # RK4 steps of the end-of-run comparison: the configuration's own count
+    # (reacting 200, Taylor-Green 100) unless given
+    n_eor = args.end_of_run if args.end_of_run is not None else (
+        200 if w["kind"] == "reacting" else 100)
+    if n_eor > 0 and world == 1 and not args.profile:
         if mixture:
-            eor = _end_of_run_mixture(dcoll, gas, gas_learn, q64, t64, args.end_of_run,
+            eor = _end_of_run_mixture(dcoll, gas, gas_learn, q64, t64, n_eor,
                                       dt=args.end_of_run_dt)
         else:
-            eor = _end_of_run(dcoll, gas, q64, args.end_of_run, w["n"])
+            eor = _end_of_run(dcoll, gas, q64, n_eor, w["n"])
         status |= runtime.read_status(dcoll, dev)
     names = [f[0] for f in forms]
     tot = _max_over_ranks([res[n][0] for n in names], dev)
@@ -997,7 +1001,7 @@ def _run_ours(args):
     # the divergence pass (node flux + surface on the split path)
     from mirgecom_b200 import runtime as _rt
     per_step = (1 if mixture else 0) + {"volume_face": 2, "gradient_volume_face": 3}.get(
-        _rt._path(dcoll), 3)
+        _rt._path(dcoll, gas), 3)
     line = {
         "metric": "DOF-RHS evals/s", "value": values[head], "unit": "DOF-RHS/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -1052,10 +1056,11 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--end-of-run", type=int, default=200,
+    ap.add_argument("--end-of-run", type=int, default=None,
                     help="after timing, run this many RK4 steps in the float64 and the "
                          "headline mixed form from the same state and report their "
-                         "per-field difference (0: skip)")
+                         "per-field difference (0: skip; default: 200 for the reacting "
+                         "workloads, 100 for Taylor-Green, the configurations' counts)")
     ap.add_argument("--end-of-run-dt", type=float, default=None,
                     help="time step of the reacting end-of-run comparison (s); default: "
                          "the state's smallest chemical time scale / 64")

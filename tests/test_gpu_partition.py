@@ -27,6 +27,17 @@ from mirgecom_b200.transport import SimpleTransport
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def _volume_face_layout():
+    """The single-domain reference through the layout the partitioned
+    phases run (the gradient, flux-volume and face kernels), so the two
+    differ by roundoff of the same arithmetic only."""
+    saved = runtime.RHS_PATH
+    runtime.RHS_PATH = "gradient_volume_face"
+    yield
+    runtime.RHS_PATH = saved
+
+
 def _partitioned_rhs(d, gas, q_glob, tseed_glob, nparts, dtype, sources):
     pds = [PartitionedDiscretization(d, r, nparts) for r in range(nparts)]
     tr = LocalTransport(nparts)
