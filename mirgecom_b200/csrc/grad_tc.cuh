@@ -234,6 +234,9 @@ struct TcGrad {
                              OFF_PERM + 64 * NFP <= 227 * 1024;
 };
 
+// the benchmark's configuration (order-3 tetrahedra, 7 species) fits
+static_assert(TcGrad<3, 3, 7>::OK, "tcgen05 gradient kernel no longer fits order-3 tets");
+
 // byte offset of element (row, k) in a canonical K-major no-swizzle operand
 __device__ __forceinline__ int canon_off(int row, int k, int lbo) {
   return (k >> 2) * lbo + (row >> 3) * 128 + (row & 7) * 16 + (k & 3) * 4;
