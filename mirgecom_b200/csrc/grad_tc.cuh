@@ -13,8 +13,9 @@
 //                        the neighbours or the boundary, and the element
 //                        geometry; they write the hi/lo copies of the A
 //                        operand [row = (field, element)][k] into one of two
-//                        shared-memory stages and arrive on full[s]; then
-//                        thread 0 waits on full[s], issues the tcgen05.mma
+//                        shared-memory stages and arrive on full[s]; after
+//                        the next tile barrier the group's last thread waits
+//                        on full[s] (complete by then), issues the tcgen05.mma
 //                        products
 //                        D[row][(r, i)] = sum_k U[row][k] W_r[i][k]  (k nodes)
 //                        D[row][(f, i)] = sum_k S[row][k] LIFT_f[i][k]
@@ -420,7 +421,8 @@ __global__ void __launch_bounds__(TcGrad<DIM, ORDER, NS>::NT, 1)
                     umma_desc(blh + bo, C::LBO_L, C::SBO), IDL, 1);
       }
     };
-    int issued = 0;
+    int issued = 0, last_issued = -1;
+    int pending = -1;          // a filled tile whose products are not issued yet
     const int first = blockIdx.x + grp * (int)gridDim.x;
     const int step = C::NGRP * (int)gridDim.x;
     if (first < ntiles) {
@@ -446,6 +448,23 @@ __global__ void __launch_bounds__(TcGrad<DIM, ORDER, NS>::NT, 1)
       // other buffer and with the shifted rows, and stage s is free
       asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "n"(GT) : "memory");
       if (pabort_s[grp]) break;
+      // the previous tile's products, issued by the group's last thread (it
+      // has no face item and one row piece at most): its wait and issue
+      // overlap the other threads' loads instead of delaying the barrier
+      if (gtid == GT - 1 && pending >= 0) {
+        const int ps = pending & 1;
+        if (!mbar_wait(full + ps, ((uint32_t)pending >> 1) & 1, abort_s)) {
+          atomicOr(a.status, ST_WAIT_TIMEOUT);
+          *abort_s = 1;
+        } else {
+          tc_fence_after();
+          issue_products(ps);
+          tc_commit(done + ps);
+          ++issued;
+          last_issued = pending;
+        }
+        pending = -1;
+      }
       const int e0 = tile * EPB;
       const int ne = imin(EPB, EOWN - e0);
       const int32_t* conn_b = conn_of(b);
@@ -589,25 +608,26 @@ __global__ void __launch_bounds__(TcGrad<DIM, ORDER, NS>::NT, 1)
       }
       fence_async_shared();
       mbar_arrive(full + s);
-      // ---- the group's thread 0 issues the tile's products once every
-      // thread of the group has arrived
-      if (gtid == 0) {
-        if (!mbar_wait(full + s, use & 1, abort_s)) {
-          atomicOr(a.status, ST_WAIT_TIMEOUT);
-          *abort_s = 1;
-        } else {
-          tc_fence_after();
-          issue_products(s);
-          tc_commit(done + s);
-          ++issued;
-        }
+      if (gtid == GT - 1) pending = it;
+    }
+    // the last tile's products (after a normal end of the loop)
+    if (gtid == GT - 1 && pending >= 0 && !*abort_s) {
+      const int ps = pending & 1;
+      if (!mbar_wait(full + ps, ((uint32_t)pending >> 1) & 1, abort_s)) {
+        atomicOr(a.status, ST_WAIT_TIMEOUT);
+        *abort_s = 1;
+      } else {
+        tc_fence_after();
+        issue_products(ps);
+        tc_commit(done + ps);
+        ++issued;
+        last_issued = pending;
       }
     }
     // on an early exit, let the products already issued finish before the
     // TMEM is released
-    if (gtid == 0 && *abort_s && issued > 0) {
-      const int lastit = grp + (issued - 1) * C::NGRP;
-      if (!mbar_wait(done + (lastit & 1), ((uint32_t)lastit >> 1) & 1, nullptr))
+    if (gtid == GT - 1 && *abort_s && issued > 0) {
+      if (!mbar_wait(done + (last_issued & 1), ((uint32_t)last_issued >> 1) & 1, nullptr))
         atomicOr(a.status, ST_WAIT_TIMEOUT);
     }
   } else {
