@@ -193,13 +193,14 @@ struct TcGrad {
   static constexpr int BV_BYTES = KV / 4 * LBO_V;
   static constexpr int BL_BYTES = KL / 4 * LBO_L;
   static constexpr int GEO = DIM * DIM + NF * DIM;    // rx, unit normals per element
-  // NGRP producer groups of GW warps, group g filling the block's tiles
-  // it = g, g + NGRP, ... (tile it into stage it % 2); four epilogue warps
-#ifndef MGC_TC_NGRP
-#define MGC_TC_NGRP 1
-#endif
-  static constexpr int NGRP = MGC_TC_NGRP;
-  static constexpr int GW = 12 / NGRP, GT = GW * 32;
+  // one producer group of GW warps filling the block's tiles (tile it into
+  // stage it % 2); four epilogue warps.  A single group is what the
+  // deferred product issue assumes: the previous tile's products are issued
+  // after the next tile's barrier, which waits for the stage of the tile
+  // before (two producer groups, each reusing its own stage, would wait for
+  // their own unissued products)
+  static constexpr int NGRP = 1;
+  static constexpr int GW = 12, GT = GW * 32;
   static constexpr int NPROD = NGRP * GT, NEPI = 128;
   // producer work items per tile and the rounds of a group they take
   static constexpr int ROW_ITEMS = NP / 4 * NU * EPB;
