@@ -1253,9 +1253,57 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT2),
     }
     __syncthreads();
 
-    // rhs += LIFT S on the tensor cores; one m-tile and NTG n-tiles per item
+    // rhs += LIFT S on the tensor cores.  float32: one item per group of NTG
+    // column tiles and every m-tile, each face value split into its tf32
+    // hi/lo words once; float64: one m-tile and NTG column tiles per item
     constexpr int NNT = NCOL / 8;
     constexpr int NTG = (NNT % 3 == 0) ? 3 : ((NNT % 2 == 0) ? 2 : 1);
+    if constexpr (V::TF32) {
+      for (int ngp = warp; ngp < NNT / NTG; ngp += nwarps) {
+        float d[MT][NTG][NACC];
+#pragma unroll
+        for (int t = 0; t < MT; ++t)
+#pragma unroll
+          for (int u = 0; u < NTG; ++u)
+#pragma unroll
+            for (int v = 0; v < NACC; ++v) d[t][u][v] = 0.f;
+        const R* bcol = bm + (ngp * NTG * 8 + gq) * KF + tq;
+#pragma unroll
+        for (int ks = 0; ks < KFR / 8; ++ks) {
+          SplitB bs[NTG];
+#pragma unroll
+          for (int u = 0; u < NTG; ++u)
+            bs[u] = SplitB(bcol[u * 8 * KF + ks * 8], bcol[u * 8 * KF + ks * 8 + 4]);
+#pragma unroll
+          for (int t = 0; t < MT; ++t) {
+            uint32_t ah[4], alo[4];
+            load_a_tf32_ldsm(ah, am, KF, t * 16, ks * 8, lane);
+            load_a_tf32_ldsm(alo, am + MP * KF, KF, t * 16, ks * 8, lane);
+#pragma unroll
+            for (int u = 0; u < NTG; ++u) mma_tf32x3(d[t][u], ah, alo, bs[u]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < NTG; ++u)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int col = (ngp * NTG + u) * 8 + 2 * tq + h;
+            const int c = col / EPB, e = col % EPB;
+            if (c >= NC || e >= ne) continue;
+            R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
+#pragma unroll
+            for (int t = 0; t < MT; ++t)
+#pragma unroll
+              for (int half = 0; half < NACC / 2; ++half) {
+                const int i = t * MROW + gq + 8 * half;
+                if (i >= NP) continue;
+                const R v = outp[i] + d[t][u][2 * half + h];
+                outp[i] = v;
+                bad |= !(v == v);
+              }
+          }
+      }
+    } else
     for (int w = warp; w < (NNT / NTG) * MT; w += nwarps) {
       const int ngp = w / MT, t = w % MT;
       R d[NTG][NACC];
