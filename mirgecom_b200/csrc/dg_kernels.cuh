@@ -632,7 +632,83 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
     }
     __syncthreads();
 
-    // phase 3: contraction and metric combination
+    // phase 3: contraction and metric combination.  float32: one item per
+    // n-tile and every m-tile, each B value split into tf32 hi/lo once
+    if constexpr (C::TF32) {
+      for (int nt = warp; nt < NCOL / 8; nt += nwarps) {
+        float du[MT][DIM][4], lf[MT][NF][4];
+#pragma unroll
+        for (int t = 0; t < MT; ++t)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) du[t][r][v] = 0.f;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) lf[t][f][v] = 0.f;
+          }
+        const R* bcol = bu + (nt * 8 + gq) * KU + tq;
+        const R* scol = bs + (nt * 8 + gq) * KS + tq;
+#pragma unroll
+        for (int ks = 0; ks < KUR / 8; ++ks) {
+          const SplitB b(bcol[ks * 8], bcol[ks * 8 + 4]);
+#pragma unroll
+          for (int t = 0; t < MT; ++t)
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) {
+              uint32_t ah[4], alo[4];
+              load_a_tf32_ldsm(ah, aw + r * MP * KU, KU, t * 16, ks * 8, lane);
+              load_a_tf32_ldsm(alo, aw + AWN + r * MP * KU, KU, t * 16, ks * 8, lane);
+              mma_tf32x3(du[t][r], ah, alo, b);
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+          for (int ks = 0; ks < NFPK / 8; ++ks) {
+            const SplitB b(scol[f * NFPK + ks * 8], scol[f * NFPK + ks * 8 + 4]);
+#pragma unroll
+            for (int t = 0; t < MT; ++t) {
+              uint32_t ah[4], alo[4];
+              load_a_tf32_ldsm(ah, al + f * MP * KL, KL, t * 16, ks * 8, lane);
+              load_a_tf32_ldsm(alo, al + ALN + f * MP * KL, KL, t * 16, ks * 8, lane);
+              mma_tf32x3(lf[t][f], ah, alo, b);
+            }
+          }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int col = nt * 8 + 2 * tq + h;
+          const int c = col / EPB, e = col % EPB;
+          if (c >= NU || e >= ne) continue;
+          R rxe[DIM][DIM], nre[NF][DIM];
+#pragma unroll
+          for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) rxe[r][j] = rx_s[e * DIM * DIM + r * DIM + j];
+#pragma unroll
+          for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) nre[f][j] = nrm_s[(e * NF + f) * DIM + j];
+          R* outp = a.out + ((int64_t)c * DIM) * EN + (int64_t)(e0 + e) * NP;
+#pragma unroll
+          for (int t = 0; t < MT; ++t)
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+              const int i = t * Tile<R>::MROW + gq + 8 * half;
+              if (i >= NP) continue;
+              const int v = 2 * half + h;
+#pragma unroll
+              for (int j = 0; j < DIM; ++j) {
+                R gsum = R(0);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) gsum += nre[f][j] * lf[t][f][v];
+#pragma unroll
+                for (int r = 0; r < DIM; ++r) gsum -= rxe[r][j] * du[t][r][v];
+                outp[(int64_t)j * EN + i] = gsum;
+              }
+            }
+        }
+      }
+    } else
     for (int w = warp; w < (NCOL / 8) * MT; w += nwarps) {
       const int nt = w / MT, t = w % MT;
       R du[DIM][NACC], lf[NF][NACC];
@@ -1415,11 +1491,60 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
     }
     __syncthreads();
 
-    // rhs = [-W | LIFT] [G ; S] on the tensor cores (+ sources); one m-tile
-    // and NTG n-tiles per warp item, so each A fragment load serves NTG
-    // products
+    // rhs = [-W | LIFT] [G ; S] on the tensor cores (+ sources).  float32:
+    // one warp item per group of NTG n-tiles and every m-tile, each B value
+    // split into its tf32 hi/lo words once; float64: one m-tile and NTG
+    // n-tiles per item, so each A fragment load serves NTG products
     constexpr int NNT = NCOL / 8;
     constexpr int NTG = (NNT % 3 == 0) ? 3 : ((NNT % 2 == 0) ? 2 : 1);
+    if constexpr (C::TF32) {
+      for (int ng = warp; ng < NNT / NTG; ng += nwarps) {
+        float d[MT][NTG][NACC];
+#pragma unroll
+        for (int t = 0; t < MT; ++t)
+#pragma unroll
+          for (int u = 0; u < NTG; ++u)
+#pragma unroll
+            for (int v = 0; v < NACC; ++v) d[t][u][v] = 0.f;
+        const R* bcol = bm + (ng * NTG * 8 + gq) * KB + tq;
+#pragma unroll 2
+        for (int ks = 0; ks < KRR / 8; ++ks) {
+          SplitB bs[NTG];
+#pragma unroll
+          for (int u = 0; u < NTG; ++u)
+            bs[u] = SplitB(bcol[u * 8 * KB + ks * 8], bcol[u * 8 * KB + ks * 8 + 4]);
+#pragma unroll
+          for (int t = 0; t < MT; ++t) {
+            uint32_t ah[4], alo[4];
+            load_a_tf32_ldsm(ah, am, KB, t * 16, ks * 8, lane);
+            load_a_tf32_ldsm(alo, am + MP * KB, KB, t * 16, ks * 8, lane);
+#pragma unroll
+            for (int u = 0; u < NTG; ++u) mma_tf32x3(d[t][u], ah, alo, bs[u]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < NTG; ++u)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int col = (ng * NTG + u) * 8 + 2 * tq + h;
+            const int c = col / EPB, e = col % EPB;
+            if (c >= NC || e >= ne) continue;
+            R* outp = a.out + (int64_t)c * EN + (int64_t)(e0 + e) * NP;
+#pragma unroll
+            for (int t = 0; t < MT; ++t)
+#pragma unroll
+              for (int half = 0; half < NACC / 2; ++half) {
+                const int i = t * Tile<R>::MROW + gq + 8 * half;
+                if (i >= NP) continue;
+                R v = d[t][u][2 * half + h];
+                if (sources && c >= 2 + DIM)
+                  v += a.srcbuf[(int64_t)(c - 2 - DIM) * EN + (int64_t)(e0 + e) * NP + i];
+                outp[i] = v;
+                bad |= !(v == v);
+              }
+          }
+      }
+    } else
     for (int w = warp; w < (NNT / NTG) * MT; w += nwarps) {
       const int ng = w / MT, t = w % MT;
       R d[NTG][NACC];
