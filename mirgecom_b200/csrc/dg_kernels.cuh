@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_GRAD))
       for (int c = 0; c < NU; ++c) {
         const R um = bu[(c * EPB + e) * KU + k];           // u- - u0
         const R u0 = u0_s[c * EPB + e];
-        const R v = (mode == 0) ? ((up[c] - u0) + um) / R(2) : up[c] - u0;
+        const R v = (mode == 0) ? ((up[c] - u0) + um) * R(0.5) : up[c] - u0;
         bcol[c * EPB * KS] = fsc * v;
       }
     }
@@ -1006,7 +1006,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB))
 #pragma unroll
           for (int j = 0; j < DIM; ++j) fvpn += fvp[c][j] * n[j];
           const R fvmn = ftm[c] + fim[c];
-          out[c] += (fvmn + fvpn) / R(2);
+          out[c] += (fvmn + fvpn) * R(0.5);
         }
       }
     }
@@ -1331,7 +1331,7 @@ __device__ __noinline__ void surface_face_general(const DGArgs<R> a, const GasPa
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       R out = -fi[c];
-      if (VISC) out += ((ftm[c] + fim[c]) + (fpn[c] + fip[c])) / R(2);
+      if (VISC) out += ((ftm[c] + fim[c]) + (fpn[c] + fip[c])) * R(0.5);
       bcol[c * cstride] = fsc * (out - f0n[c]);
     }
   }
@@ -1479,7 +1479,7 @@ __global__ void __launch_bounds__(256, (Cfg<R, DIM, ORDER, NS, MIX>::MINB_SURF))
               s0 += f0v[cc * DIM + j] * n[j];
             }
             const R dq = a.q[c * EN + gm] - a.q[c * EN + gi];
-            const R out = (sm_ + sp_) / R(2) - lam * dq / R(2);
+            const R out = (sm_ + sp_) * R(0.5) - lam * dq * R(0.5);
             bcol[c * EPB * KB] = fsc * (out - s0);
           }
         }

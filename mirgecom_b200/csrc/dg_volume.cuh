@@ -475,7 +475,7 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT),
         for (int c = 0; c < NU; ++c) {
           const R um = bu[(c * EPB + e) * KU + k];
           const R u0 = u0_s[c * EPB + e];
-          const R v = (mode == 0) ? ((up[c] - u0) + um) / R(2) : up[c] - u0;
+          const R v = (mode == 0) ? ((up[c] - u0) + um) * R(0.5) : up[c] - u0;
           bcol[c * EPB * KS] = fsc * v;
         }
       }
@@ -1121,7 +1121,7 @@ __device__ __noinline__ void face_flux_general(const DGArgs<R> a, int64_t EN, in
   for (int c = 0; c < NC; ++c) {
     R out = -fi[c];
     // F_V . n = F . n + F_I . n on each side; the neighbour record holds -F . n
-    if (VISC) out += ((recm[c] + fim[c]) + (-recp[c] + fip[c])) / R(2);
+    if (VISC) out += ((recm[c] + fim[c]) + (-recp[c] + fip[c])) * R(0.5);
     bcol[c * cstride] = fsc * (out - s0[c]);
   }
 }
@@ -1247,7 +1247,7 @@ __global__ void __launch_bounds__((VCfg<R, DIM, ORDER, NS, MIX>::NT2),
       const R lam = (a.flux_kind == FLUX_RUSANOV) ? fmax(rm[NC], rp[NC]) : R(0);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        const R out = (rm[c] - rp[c]) / R(2) - lam * (qm[c] - qp[c]) / R(2);
+        const R out = (rm[c] - rp[c]) * R(0.5) - lam * (qm[c] - qp[c]) * R(0.5);
         bcol[c * EPB * KF] = fsc * (out - sh[c]);
       }
     }

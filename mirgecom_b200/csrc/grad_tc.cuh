@@ -587,7 +587,7 @@ __global__ void __launch_bounds__(TcGrad<DIM, ORDER, NS>::NT, 1)
           const float um = raw[(c * EPB + e) * NP + k];
           float v;
           if (mode == 0)
-            v = ((nb[j][c] - u0) + um) / 2.f;
+            v = ((nb[j][c] - u0) + um) * 0.5f;
           else if (mode == 1)
             v = nb[j][c] - u0;
           else

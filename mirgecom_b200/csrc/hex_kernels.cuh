@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(256, 2) k_hex_grad(DGArgs<R> a, GasParams g) {
       for (int c = 0; c < NU; ++c) {
         const R u0 = u_s[(e * NU + c) * NP];
         const R um = u_s[(e * NU + c) * NP + k] - u0;
-        scol[c * NFN] = (mode == 0) ? ((up[c] - u0) + um) / R(2) : up[c] - u0;
+        scol[c * NFN] = (mode == 0) ? ((up[c] - u0) + um) * R(0.5) : up[c] - u0;
       }
     }
     __syncthreads();
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(256, 2) k_hex_surface(DGArgs<R> a, GasParams g
               s0 += f0v[cc * DIM + j] * n[j];
             }
             const R dq = a.q[c * EN + gm] - a.q[c * EN + gi];
-            const R out = (sm_ + sp_) / R(2) - lam * dq / R(2);
+            const R out = (sm_ + sp_) * R(0.5) - lam * dq * R(0.5);
             bcol[c * NFN] = fsc * (out - s0);
           }
         }
