@@ -381,7 +381,10 @@ __global__ void __launch_bounds__(TcGrad<DIM, ORDER, NS>::NT, 1)
         }
         const float mag = sqrtf(mag2);
 #pragma unroll
-        for (int j = 0; j < DIM; ++j) pg[DIM * DIM + f * DIM + j] = nv[j] / mag;
+        // approximate quotient: an IEEE division site (with its out-of-line
+        // slow path) cost this whole kernel 1.1 ms at 80^3; the normals
+        // differ from the other kernels' by a few ulp
+        for (int j = 0; j < DIM; ++j) pg[DIM * DIM + f * DIM + j] = __fdividef(nv[j], mag);
         fs_of(b)[gi] = mag * RefBank<float>::get(S::OFF_FSR + f);
         if (f == 0) {
 #pragma unroll
